@@ -1,0 +1,174 @@
+/*
+ * qmcrt.h - C ABI of the B200 quasi-Monte-Carlo heliostat-field ray tracer.
+ *
+ * A drop-in for the QuasiMonteCarloRayTracer path of SolarEnergy_Chier: the
+ * same .scn scene files, JSON configuration files and heliostat-index task
+ * files, the same SolarScene / RayTracingPipeline steps, the same flux-map
+ * text output.  Plain pointers and sizes only; every call returns a status
+ * (QMCRT_OK or an error code) and qmcrt_last_error() gives the message of the
+ * last failure on the calling thread.  No C++ exception crosses this
+ * boundary.  Streams are passed as `void*` holding a cudaStream_t (NULL =
+ * the legacy default stream).  A scene is owned by one host thread at a time.
+ *
+ * Each declaration names the reference interface it replaces
+ * (file:line within the SolarEnergy_Chier tree).
+ */
+#ifndef QMCRT_H
+#define QMCRT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QMCRT_OK 0
+#define QMCRT_ERR_INVALID 1   /* bad argument or index (reference: std::runtime_error)   */
+#define QMCRT_ERR_IO 2        /* unreadable or malformed file (reference: false + cerr)  */
+#define QMCRT_ERR_CUDA 3      /* CUDA runtime failure (reference: exit(1))               */
+#define QMCRT_ERR_STATE 4     /* call out of order, e.g. no sample pool yet              */
+
+typedef struct qmcrt_scene qmcrt_scene;
+
+/* Message of the last failed call on this thread ("" when none). */
+const char* qmcrt_last_error(void);
+int qmcrt_version(void);
+
+/* ---- scene --------------------------------------------------------------
+ * Replaces SceneConfiguration::getInstance()->loadConfiguration
+ * (Scene/SceneConfiguration.cpp:39-69), SceneLoader::SceneFileRead
+ * (Scene/SceneLoader.cpp:243-353) and the geometry half of
+ * SceneProcessor::processScene (Scene/SceneProcessor.cpp:9-39): loads both
+ * files, builds receivers, grid cell lists, heliostat normals and
+ * sub-heliostat tables, and uploads them to `device`.  The sample pools and
+ * facet offsets (the cuRAND half of processScene, Scene/SceneProcessor.cu:147-271
+ * and Heliostat.cu:57-62) are generated with `seed` by the scrambled Sobol
+ * generator; qmcrt_set_sample_pool / qmcrt_set_facet_offsets replace them.
+ * device = -1 loads host-only: the processed geometry can be inspected with
+ * the getters below on a machine without a GPU, every device call fails with
+ * QMCRT_ERR_STATE. */
+int qmcrt_scene_load(const char* scene_path, const char* config_path, int device, unsigned seed,
+                     qmcrt_scene** out);
+/* Replaces SolarScene::clear (Scene/SolarScene.cpp:31-46). */
+void qmcrt_scene_free(qmcrt_scene* scene);
+
+typedef struct {
+  int num_receivers, num_grids, num_heliostats;
+  int num_sunshape_groups, num_per_sunshape_group, pool_size;
+  int inverse_transform_sampling_groups, config_fields;
+  float sun_dir[3];
+  float dni, csr, receiver_pixel_length, helio_disturb_std, helio_pixel_length, helio_reflected_rate;
+  float ground_length, ground_width;
+  long long total_facets;
+} qmcrt_scene_info;
+/* SolarScene / SceneConfiguration getters (Scene/SolarScene.h:35-58, Scene/SceneConfiguration.h:20-33). */
+int qmcrt_scene_get_info(const qmcrt_scene* scene, qmcrt_scene_info* info);
+
+/* Receiver state after CInit (Scene/DataStructure/Receiver/Receiver.cuh:11-86):
+ * vertices12 = 4 world vertices (rectangle), normal3 (normalised), focus3
+ * (rectangle focus centre). */
+int qmcrt_receiver_get(const qmcrt_scene* scene, int receiver, int* type, int* width, int* height,
+                       float* pixel_length, float* vertices12, float* normal3, float* focus3);
+/* Heliostat state after CSetNormalAndRotate (Scene/DataStructure/Heliostat/Heliostat.cuh:18-90). */
+int qmcrt_heliostat_get(const qmcrt_scene* scene, int heliostat, int* type, int* grid, int* num_facets,
+                        int* num_sub, int* sub_begin, float* pos3, float* size3, float* normal3,
+                        float* focus_length);
+/* Grid after Cinit + CGridHelioMatch (Scene/DataStructure/Grid/RectangleGrid.cu:8-117):
+ * cells3, sub-heliostat count, CSR non-zeros, receiver, first heliostat, heliostat count. */
+int qmcrt_grid_get(const qmcrt_scene* scene, int grid, int* cells3, int* num_sub, int* nnz, int* receiver,
+                   int* start, int* count);
+/* The grid's cell lists in the reference layout (d_grid_helio_index_,
+ * d_grid_helio_match_; RectangleGrid.cuh:49-52): index has cells+1 entries. */
+int qmcrt_grid_csr(const qmcrt_scene* scene, int grid, int* index, int* match);
+/* Sub-heliostat vertex table of a grid, 9 floats per sub-heliostat
+ * (QuasiMonteCarloRayTracer::setFlatRectangleHeliostatVertexs, QuasiMonteCarloRayTracer.cpp:182-209). */
+int qmcrt_grid_vertices(const qmcrt_scene* scene, int grid, float* xyz);
+/* Micro-facet centres and normals of a heliostat, 3 floats each, computed on
+ * the device by the tracer's facet function (replaces
+ * Heliostat::CGetDiscreteMicroHelioOriginsAndNormals, RectangleHelio.cu:84-116,
+ * FocusFlatRectangleHelio.cu:68-116).  Host output buffers. */
+int qmcrt_heliostat_facets(qmcrt_scene* scene, int heliostat, float* origins, float* normals);
+
+/* ---- sampling ------------------------------------------------------------
+ * Injection point for parity runs (the pool replacement of
+ * Tests/QuasiMonteCarloRayTracingTests/receiverIntersectUtil.cpp:8-33):
+ * dirs_xyz and perturb_xyz hold groups*per_group float3 each, host memory
+ * (on_device = 0) or device memory (on_device = 1). */
+int qmcrt_set_sample_pool(qmcrt_scene* scene, const float* dirs_xyz, const float* perturb_xyz, int groups,
+                          int per_group, int on_device);
+/* Regenerates both pools on the device (replaces SceneProcessor::set_samplelights
+ * and set_perturbation, Scene/SceneProcessor.cu:147-271).  sunshape 0 = Buie
+ * from the configuration's csr (the reference's inverse CDF), 1 = pillbox of
+ * half-angle `half_angle` radians.  Slope error sigma = helio_disturb_std. */
+int qmcrt_generate_sample_pool(qmcrt_scene* scene, unsigned seed, int sunshape, float half_angle);
+/* Reads back the pools (pool_size float3 each) into host buffers. */
+int qmcrt_get_sample_pool(qmcrt_scene* scene, float* dirs_xyz, float* perturb_xyz);
+/* Per-facet pool offsets of one heliostat (the d_microHelio_groups array,
+ * Heliostat::generateDeviceMicrohelioGroup, Heliostat.cu:57-62).  n must be
+ * num_facets (entry num_facets is then set to offsets[0]) or num_facets + 1
+ * (the extra entry is what the reference's kernel reads for the last facet). */
+int qmcrt_set_facet_offsets(qmcrt_scene* scene, int heliostat, const int* offsets, int n);
+int qmcrt_get_facet_offsets(qmcrt_scene* scene, int heliostat, int* offsets, int n);
+int qmcrt_generate_facet_offsets(qmcrt_scene* scene, unsigned seed);
+
+/* exact = 1 selects the kernel build without FMA contraction (every float
+ * operation rounded as the CPU oracle rounds it); 0 (default) the production build. */
+int qmcrt_set_math_mode(qmcrt_scene* scene, int exact);
+/* Trace only light indexes [begin, end) of every facet (default [0, per_group)).
+ * Energies keep the full-trace factor DNI*(hpx/rpx)^2*rho/per_group. */
+int qmcrt_set_light_range(qmcrt_scene* scene, int begin, int end);
+
+/* ---- tracing -------------------------------------------------------------
+ * Replaces QuasiMonteCarloRayTracer::rayTracing(SolarScene*, int)
+ * (QuasiMonteCarloRayTracing/QuasiMonteCarloRayTracer.cpp:15-91): adds the
+ * heliostat's flux into its receiver's image (images accumulate until
+ * cleared) and its FP64 power into the per-heliostat total.  Asynchronous on
+ * `stream`.  Invalid indexes fail as checkValidHeliostatIndex (:96-127) does. */
+int qmcrt_trace_heliostat(qmcrt_scene* scene, int heliostat, void* stream);
+/* All listed heliostats in one launch (the loop of RayTracingPipeline.cpp:66-81). */
+int qmcrt_trace_heliostats(qmcrt_scene* scene, const int* heliostats, int n, void* stream);
+
+/* Receiver image, resolution.y rows of resolution.x floats
+ * (Receiver::getDeviceImage, Receiver.cuh:69-75).  `out` is host memory;
+ * the call synchronises the scene's device. */
+int qmcrt_receiver_image(qmcrt_scene* scene, int receiver, float* out, int* width, int* height);
+int qmcrt_receiver_device_image(qmcrt_scene* scene, int receiver, float** device_ptr, int* width, int* height);
+/* Replaces Receiver::Cclean_image_content (Scene/DataStructure/Receiver/Receiver.cu:33-45). */
+int qmcrt_receiver_clear(qmcrt_scene* scene, int receiver, void* stream);
+/* FP64 per-heliostat energy and total accumulated by the tracer since the
+ * last qmcrt_power_clear (per_heliostat: num_heliostats doubles, may be NULL). */
+int qmcrt_power_fp64(qmcrt_scene* scene, double* per_heliostat, double* total);
+int qmcrt_power_clear(qmcrt_scene* scene);
+/* Counters: [0] receiver hits clamped into the image (u or v == 1),
+ * [1] grid walks stopped by the step bound, [2..3] reserved. */
+int qmcrt_diagnostics(qmcrt_scene* scene, unsigned long long* out4);
+
+/* Per-ray outcome for facets [facet_begin, facet_end) x lights [light_begin,
+ * light_end) of one heliostat, row-major by facet: pixel index for a
+ * receiver hit, -1 shadowed, -2 blocked, -3 missed the receiver.  Traces into
+ * scratch; scene images and powers are untouched. */
+int qmcrt_debug_hit_records(qmcrt_scene* scene, int heliostat, int facet_begin, int facet_end,
+                            int light_begin, int light_end, int* codes);
+
+/* ---- smoothing and output ------------------------------------------------
+ * Replaces ImageSmoother::image_smooth (Tool/Smoother/ImageSmoother.cu:68-113):
+ * in-place trimmed mean of a device image.  0 <= trim_ratio < 0.5. */
+int qmcrt_smooth(float* device_image, int width, int height, int radius, float trim_ratio, void* stream);
+
+/* Replaces TaskLoader::loadRayTracingHeliostatIndex (RayTracingPipeline/TaskLoader.cpp:114-204).
+ * status: 1 true, 0 false (repeated or surplus indexes).  receivers receives the
+ * grid ids of the listed heliostats, as the reference records them. */
+int qmcrt_load_tasks(const qmcrt_scene* scene, const char* path, int* heliostats, int* num_heliostats,
+                     int capacity, int* receivers, int* num_receivers, int* status);
+
+/* Replaces ImageSaver::saveText (Tool/ImageSaver/ImageSaver.cpp:13-58). */
+int qmcrt_save_text(const char* path, int height, int width, const float* host_data, int precision,
+                    float* max_value);
+
+/* Replaces RayTracingPipeline::rayTracing(argc, argv) (RayTracingPipeline/RayTracingPipeline.cpp:16-114),
+ * getopt flags -c -s -o -h (Tool/ArgumentParser/ArgumentParser.cpp:49-94). */
+int qmcrt_pipeline_run(int argc, char** argv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QMCRT_H */

@@ -1,0 +1,109 @@
+"""In-tree build of the native library and the drop-in executable.
+
+Produces, next to this file:
+  libqmcrt.so   the C ABI of include/qmcrt.h (host C++ + sm_100a kernels)
+  bin/qmcrt     the RayTracingPipeline command-line executable
+
+Host C++ is compiled by g++ with -ffp-contract=off so that the scene
+geometry rounds exactly as the reference's host code does.  The tracer is
+compiled twice: with FMA contraction (production) and with -fmad=false (every
+float operation rounded like the CPU oracle).  Only nvcc and g++ are needed;
+the build works on a machine without a GPU.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+OBJ = PKG / "_build"
+LIB = PKG / "libqmcrt.so"
+EXE = PKG / "bin" / "qmcrt"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+NVCC = str(CUDA_HOME / "bin" / "nvcc")
+
+HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-unused-function"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-ffp-contract=off"] + ARCH
+
+HOST_SOURCES = ["scene.cpp", "buie_table.cpp", "capi.cpp", "pipeline.cpp"]
+CUDA_UNITS = [
+    ("tracer.cu", "tracer_fast.o", ["-DQM_TRACE_VARIANT=fast"]),
+    ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-fmad=false"]),
+    ("pools.cu", "pools.o", []),
+    ("smooth.cu", "smooth.o", []),
+]
+
+
+def _run(cmd: list[str]) -> None:
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        sys.stderr.write(proc.stdout + proc.stderr)
+        raise RuntimeError("build step failed: " + " ".join(cmd))
+
+
+def _digest(paths: list[Path], extra: list[str]) -> str:
+    h = hashlib.sha256()
+    for p in paths:
+        h.update(p.read_bytes())
+    h.update(" ".join(extra).encode())
+    return h.hexdigest()
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every unit whose inputs changed and link libqmcrt.so and bin/qmcrt."""
+    OBJ.mkdir(exist_ok=True)
+    EXE.parent.mkdir(exist_ok=True)
+    headers = sorted(CSRC.glob("*.h")) + [INCLUDE / "qmcrt.h"]
+    objects = []
+    for src in HOST_SOURCES:
+        obj = OBJ / (Path(src).stem + ".o")
+        cmd = ["g++", *HOST_FLAGS, f"-I{CSRC}", f"-I{INCLUDE}", f"-I{CUDA_HOME / 'include'}", "-c",
+               str(CSRC / src), "-o", str(obj)]
+        _compile(obj, [CSRC / src, *headers], cmd, force, verbose)
+        objects.append(obj)
+    for src, name, flags in CUDA_UNITS:
+        obj = OBJ / name
+        cmd = [NVCC, *NVCC_FLAGS, *flags, f"-I{CSRC}", f"-I{INCLUDE}", "-c", str(CSRC / src), "-o", str(obj)]
+        _compile(obj, [CSRC / src, *headers], cmd, force, verbose)
+        objects.append(obj)
+    link = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objects), "-lcudart"]
+    _link(LIB, objects, link, force, verbose)
+    main_obj = OBJ / "main.o"
+    _compile(main_obj, [CSRC / "main.cpp", INCLUDE / "qmcrt.h"],
+             ["g++", *HOST_FLAGS, f"-I{INCLUDE}", "-c", str(CSRC / "main.cpp"), "-o", str(main_obj)], force, verbose)
+    _link(EXE, [main_obj, LIB], ["g++", "-o", str(EXE), str(main_obj), f"-L{PKG}", "-lqmcrt",
+                                  f"-Wl,-rpath,$ORIGIN/..", f"-L{CUDA_HOME / 'lib64'}", "-lcudart"], force, verbose)
+    return LIB
+
+
+def _compile(obj: Path, inputs: list[Path], cmd: list[str], force: bool, verbose: bool) -> None:
+    stamp = obj.with_suffix(obj.suffix + ".sha")
+    digest = _digest(inputs, cmd)
+    if not force and obj.exists() and stamp.exists() and stamp.read_text() == digest:
+        return
+    if verbose:
+        print(" ".join(cmd))
+    _run(cmd)
+    stamp.write_text(digest)
+
+
+def _link(out: Path, inputs: list[Path], cmd: list[str], force: bool, verbose: bool) -> None:
+    if not force and out.exists() and all(out.stat().st_mtime >= p.stat().st_mtime for p in inputs):
+        return
+    if verbose:
+        print(" ".join(cmd))
+    _run(cmd)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True)
+    print(LIB)

@@ -1,0 +1,963 @@
+// C ABI (include/qmcrt.h) over the host scene model and the sm_100a kernels.
+#include "qmcrt.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "device_scene.h"
+#include "pools.h"
+#include "sampling.h"
+#include "scene.h"
+#include "smooth.h"
+#include "tracer.h"
+#include "vecmath.h"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct ApiError : std::runtime_error {
+  int code;
+  ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw ApiError(QMCRT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return QMCRT_OK;
+  } catch (const ApiError& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return QMCRT_ERR_CUDA;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return QMCRT_ERR_INVALID;
+  }
+}
+
+[[noreturn]] void invalid(const std::string& m) { throw ApiError(QMCRT_ERR_INVALID, m); }
+
+// Device buffer owned by the scene.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t n) {
+    if (n == bytes && p) return;
+    release();
+    if (n == 0) return;
+    cuda_check(cudaMalloc(&p, n), "cudaMalloc");
+    bytes = n;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+template <class T>
+void upload(DBuf& b, const std::vector<T>& v) {
+  b.alloc(v.size() * sizeof(T));
+  if (!v.empty()) cuda_check(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+}
+
+struct GridBufs {
+  DBuf hindex, hmatch, bound, hsub, subv;
+};
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev_);
+    if (prev_ != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+    switched_ = prev_ != dev;
+  }
+  ~DeviceGuard() {
+    if (switched_) cudaSetDevice(prev_);
+  }
+
+ private:
+  int prev_ = 0;
+  bool switched_ = false;
+};
+
+}  // namespace
+
+struct qmcrt_scene {
+  int device = 0;
+  unsigned seed = 0;
+  qm::SceneModel model;
+  std::vector<std::unique_ptr<GridBufs>> grid_bufs;
+  std::vector<qm::DevGrid> grids;
+  DBuf d_grids;
+  std::vector<std::unique_ptr<DBuf>> images;
+  std::vector<qm::DevReceiver> receivers;
+  DBuf d_receivers;
+  DBuf d_local;  // focus-flat local centres then normals
+  std::vector<long long> local_base;
+  DBuf d_offsets;
+  std::vector<long long> offset_base;
+  DBuf d_samples, d_perturb;
+  int pool_size = 0;
+  DBuf d_power, d_diag;
+  std::vector<qm::DevTask> templates;
+  DBuf d_tasks, d_prefix;
+  std::vector<int> cached_ids;
+  bool cache_valid = false;
+  qm::DevTask* h_stage = nullptr;  // pinned staging for task uploads
+  long long* h_prefix = nullptr;
+  size_t stage_cap = 0;
+  cudaEvent_t stage_done = nullptr;
+  qm::SunFrame sun{};
+  int exact = 0;
+  int light_begin = 0, light_end = 0;
+  long long total_facets = 0;
+
+  ~qmcrt_scene() {
+    if (device < 0) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    cudaDeviceSynchronize();
+    if (h_stage) cudaFreeHost(h_stage);
+    if (h_prefix) cudaFreeHost(h_prefix);
+    if (stage_done) cudaEventDestroy(stage_done);
+    grid_bufs.clear();
+    images.clear();
+    d_grids.release();
+    d_receivers.release();
+    d_local.release();
+    d_offsets.release();
+    d_samples.release();
+    d_perturb.release();
+    d_power.release();
+    d_diag.release();
+    d_tasks.release();
+    d_prefix.release();
+    cudaSetDevice(prev);
+  }
+};
+
+namespace {
+
+using qm::DevGrid;
+using qm::DevReceiver;
+using qm::DevTask;
+
+// Padded bounding box of one heliostat in its own frame, from the corners of
+// all its sub-heliostat parallelograms (double precision, then widened).
+void heliostat_box(const qm::HeliostatModel& h, const std::vector<float3>& verts, float4 out[4]) {
+  double n[3] = {h.normal.x, h.normal.y, h.normal.z};
+  double nl = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+  if (!(nl > 0)) {
+    n[0] = 0;
+    n[1] = 1;
+    n[2] = 0;
+    nl = 1;
+  }
+  for (double& x : n) x /= nl;
+  double e1[3];
+  if (std::fabs(n[0]) < 0.9) {
+    // e1 = normalize(cross((1,0,0), n))
+    e1[0] = 0;
+    e1[1] = -n[2];
+    e1[2] = n[1];
+  } else {
+    // e1 = normalize(cross((0,0,1), n))
+    e1[0] = -n[1];
+    e1[1] = n[0];
+    e1[2] = 0;
+  }
+  double l1 = std::sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+  for (double& x : e1) x /= l1;
+  double e3[3] = {e1[1] * n[2] - e1[2] * n[1], e1[2] * n[0] - e1[0] * n[2], e1[0] * n[1] - e1[1] * n[0]};
+  const double* ax[3] = {e1, n, e3};
+  const double c0[3] = {h.pos.x, h.pos.y, h.pos.z};
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  double maxabs = std::fabs(c0[0]) + std::fabs(c0[1]) + std::fabs(c0[2]);
+  for (int s = h.sub_begin; s < h.sub_begin + h.num_sub; ++s) {
+    const float3 B = verts[3 * s], A = verts[3 * s + 1], C = verts[3 * s + 2];
+    const double a[3] = {A.x, A.y, A.z};
+    const double ab[3] = {(double)B.x - A.x, (double)B.y - A.y, (double)B.z - A.z};
+    const double ac[3] = {(double)C.x - A.x, (double)C.y - A.y, (double)C.z - A.z};
+    for (int corner = 0; corner < 4; ++corner) {
+      double p[3];
+      for (int i = 0; i < 3; ++i)
+        p[i] = a[i] + ((corner & 1) ? ab[i] : 0.0) + ((corner & 2) ? ac[i] : 0.0) - c0[i];
+      for (int k = 0; k < 3; ++k) {
+        double d = p[0] * ax[k][0] + p[1] * ax[k][1] + p[2] * ax[k][2];
+        lo[k] = std::min(lo[k], d);
+        hi[k] = std::max(hi[k], d);
+      }
+      maxabs = std::max(maxabs, std::fabs(p[0] + c0[0]) + std::fabs(p[1] + c0[1]) + std::fabs(p[2] + c0[2]));
+    }
+  }
+  // Padding: 1 cm plus 1e-5 of the coordinate scale, two orders of magnitude
+  // above the float rounding of the parallelogram test at that scale.
+  const double margin = 0.01 + 1e-5 * maxabs;
+  double centre[3] = {c0[0], c0[1], c0[2]};
+  double half[3];
+  for (int k = 0; k < 3; ++k) {
+    double mid = 0.5 * (lo[k] + hi[k]);
+    for (int i = 0; i < 3; ++i) centre[i] += mid * ax[k][i];
+    half[k] = 0.5 * (hi[k] - lo[k]) + margin;
+  }
+  out[0] = make_float4((float)centre[0], (float)centre[1], (float)centre[2], 0.0f);
+  for (int k = 0; k < 3; ++k)
+    out[1 + k] = make_float4((float)ax[k][0], (float)ax[k][1], (float)ax[k][2], (float)(half[k] * (1 + 1e-6)));
+}
+
+void build_device_scene(qmcrt_scene* s) {
+  qm::SceneModel& m = s->model;
+  const qm::SceneConfig& cfg = m.config;
+  if (cfg.num_sunshape_groups <= 0 || cfg.num_per_sunshape_group <= 0) invalid("sun-shape pool size must be positive");
+  long long P = (long long)cfg.num_sunshape_groups * cfg.num_per_sunshape_group;
+  if (P > (1LL << 30)) invalid("sun-shape pool is larger than 2^30 samples");
+  s->pool_size = (int)P;
+  s->light_begin = 0;
+  s->light_end = cfg.num_per_sunshape_group;
+
+  // Grids.
+  s->grid_bufs.clear();
+  s->grids.clear();
+  for (auto& g : m.grids) {
+    auto gb = std::make_unique<GridBufs>();
+    upload(gb->hindex, g.cell_hindex);
+    upload(gb->hmatch, g.cell_hmatch);
+    std::vector<float4> bound(4 * (size_t)g.num_heliostats);
+    std::vector<int2> hsub(g.num_heliostats);
+    for (int i = 0; i < g.num_heliostats; ++i) {
+      const qm::HeliostatModel& h = m.heliostats[g.start_heliostat + i];
+      hsub[i] = make_int2(h.sub_begin, h.num_sub);
+      heliostat_box(h, g.sub_vertices, &bound[4 * (size_t)i]);
+    }
+    upload(gb->bound, bound);
+    upload(gb->hsub, hsub);
+    std::vector<float4> subv(3 * (size_t)g.num_subheliostats);
+    for (int sidx = 0; sidx < g.num_subheliostats; ++sidx) {
+      const float3 B = g.sub_vertices[3 * sidx], A = g.sub_vertices[3 * sidx + 1], C = g.sub_vertices[3 * sidx + 2];
+      const float3 ab = qm::sub(B, A), ac = qm::sub(C, A);
+      subv[3 * sidx] = make_float4(A.x, A.y, A.z, ab.x);
+      subv[3 * sidx + 1] = make_float4(ab.y, ab.z, ac.x, ac.y);
+      subv[3 * sidx + 2] = make_float4(ac.z, 0.f, 0.f, 0.f);
+    }
+    upload(gb->subv, subv);
+    DevGrid dg;
+    dg.pos = g.pos;
+    dg.interval = g.interval;
+    dg.cells = g.cells;
+    dg.max_steps = g.cells.x + g.cells.y + g.cells.z + 2;
+    dg.hindex = gb->hindex.as<int>();
+    dg.hmatch = gb->hmatch.as<int>();
+    dg.bound = gb->bound.as<float4>();
+    dg.hsub = gb->hsub.as<int2>();
+    dg.subv = gb->subv.as<float4>();
+    s->grids.push_back(dg);
+    s->grid_bufs.push_back(std::move(gb));
+  }
+  upload(s->d_grids, s->grids);
+
+  // Receivers and images.
+  s->images.clear();
+  s->receivers.clear();
+  for (auto& r : m.receivers) {
+    auto img = std::make_unique<DBuf>();
+    size_t n = (size_t)std::max(r.resolution.x, 0) * std::max(r.resolution.y, 0);
+    img->alloc(std::max<size_t>(n, 1) * sizeof(float));
+    cuda_check(cudaMemset(img->p, 0, img->bytes), "cudaMemset");
+    DevReceiver dr{};
+    dr.type = r.type;
+    dr.resolution = r.resolution;
+    dr.image = img->as<float>();
+    if (r.type == 0) {
+      dr.a = r.vertex[0];
+      dr.ab = qm::sub(r.vertex[1], r.vertex[0]);
+      dr.ac = qm::sub(r.vertex[3], r.vertex[0]);
+    }
+    dr.pos = r.pos;
+    dr.size = r.size;
+    s->receivers.push_back(dr);
+    s->images.push_back(std::move(img));
+  }
+  upload(s->d_receivers, s->receivers);
+
+  // Focus-flat local facet frames.
+  std::vector<float3> local;
+  s->local_base.assign(m.heliostats.size(), -1);
+  for (size_t i = 0; i < m.heliostats.size(); ++i) {
+    const auto& h = m.heliostats[i];
+    if (h.type != 1) continue;
+    s->local_base[i] = (long long)local.size();
+    local.insert(local.end(), h.local_centers.begin(), h.local_centers.end());
+    local.insert(local.end(), h.local_normals.begin(), h.local_normals.end());
+  }
+  upload(s->d_local, local);
+
+  // Pool offsets: num_facets + 1 per heliostat in one buffer.
+  s->offset_base.assign(m.heliostats.size(), 0);
+  long long total = 0;
+  s->total_facets = 0;
+  for (size_t i = 0; i < m.heliostats.size(); ++i) {
+    s->offset_base[i] = total;
+    total += (long long)m.heliostats[i].num_facets + 1;
+    s->total_facets += m.heliostats[i].num_facets;
+  }
+  s->d_offsets.alloc((size_t)total * sizeof(int));
+
+  s->d_samples.alloc((size_t)P * sizeof(float4));
+  s->d_perturb.alloc((size_t)P * sizeof(float4));
+  s->d_power.alloc(std::max<size_t>(m.heliostats.size(), 1) * sizeof(double));
+  cuda_check(cudaMemset(s->d_power.p, 0, s->d_power.bytes), "cudaMemset");
+  s->d_diag.alloc(qm::kDiagSlots * sizeof(unsigned long long));
+  cuda_check(cudaMemset(s->d_diag.p, 0, s->d_diag.bytes), "cudaMemset");
+
+  // Sun frame of -sun_dir (QuasiMonteCarloRayTracer::generateSunrayArgument feeds
+  // -sunray_direction to local2world_rotate per ray; the frame is constant).
+  qm::Frame f = qm::make_frame(qm::neg(cfg.sun_dir), false);
+  s->sun.u = f.u;
+  s->sun.n = f.n;
+  s->sun.v = f.v;
+  s->sun.identity = f.identity ? 1 : 0;
+
+  // Per-heliostat task templates.
+  s->templates.assign(m.heliostats.size(), DevTask{});
+  for (size_t i = 0; i < m.heliostats.size(); ++i) {
+    const auto& h = m.heliostats[i];
+    const auto& g = m.grids[h.grid];
+    const auto& r = m.receivers[g.receiver];
+    DevTask t{};
+    t.type = h.type;
+    t.grid = h.grid;
+    t.receiver = g.receiver;
+    t.own = (int)i - g.start_heliostat;
+    t.num_facets = h.num_facets;
+    t.power_slot = (int)i;
+    t.row_col = h.row_col;
+    t.sub_row_col = h.sub_row_col;
+    t.pixel_length = h.pixel_length;
+    // QuasiMonteCarloRayTracer::rayTracing (QuasiMonteCarloRayTracer.cpp:58-60).
+    float ratio = h.pixel_length / r.pixel_length;
+    t.factor = cfg.dni * ratio * ratio * cfg.helio_reflected_rate / float(cfg.num_per_sunshape_group);
+    t.gap = h.gap;
+    t.sub_length = h.sub_length;
+    t.size = h.size;
+    t.pos = h.pos;
+    t.normal = h.normal;
+    qm::Frame hf = qm::make_frame(h.normal, h.type == 1);
+    t.fu = hf.u;
+    t.fn = hf.n;
+    t.fv = hf.v;
+    t.frame_identity = hf.identity ? 1 : 0;
+    if (h.type == 1) {
+      const float3* base = s->d_local.as<float3>() + s->local_base[i];
+      t.local_centers = base;
+      t.local_normals = base + h.local_centers.size();
+    }
+    t.offsets = s->d_offsets.as<int>() + s->offset_base[i];
+    s->templates[i] = t;
+  }
+  s->cache_valid = false;
+}
+
+void generate_offsets(qmcrt_scene* s, unsigned seed) {
+  for (size_t i = 0; i < s->model.heliostats.size(); ++i) {
+    long long n = (long long)s->model.heliostats[i].num_facets + 1;
+    cuda_check(qm::launch_offsets(s->d_offsets.as<int>() + s->offset_base[i], n, seed, (int)i, s->pool_size, 0),
+               "offsets kernel");
+  }
+  cuda_check(cudaDeviceSynchronize(), "offsets kernel");
+}
+
+void generate_pool(qmcrt_scene* s, unsigned seed, int sunshape, float half_angle) {
+  const qm::SceneConfig& cfg = s->model.config;
+  qm::PoolParams p{};
+  p.samples = s->d_samples.as<float4>();
+  p.perturbations = s->d_perturb.as<float4>();
+  p.pool_size = s->pool_size;
+  p.sunshape = sunshape;
+  p.half_angle = half_angle;
+  p.sigma = cfg.helio_disturb_std;
+  p.seed_sun = qm::mix32(seed * 2654435761u + 1u);
+  p.seed_slope = qm::mix32(seed * 2654435761u + 2u);
+  DBuf cdf, kk;
+  if (sunshape == qm::kSunshapeBuie) {
+    if (cfg.inverse_transform_sampling_groups <= 0) invalid("inverse_transform_sampling_groups must be positive");
+    qm::BuieHost t = qm::build_buie_table(cfg.csr, cfg.inverse_transform_sampling_groups);
+    upload(cdf, t.cdf);
+    upload(kk, t.k);
+    p.buie.cdf = cdf.as<float2>();
+    p.buie.k = kk.as<float>();
+    p.buie.n = cfg.inverse_transform_sampling_groups;
+    p.buie.less_465 = t.less_465;
+    p.buie.gamma = t.gamma;
+    p.buie.A = t.A;
+    p.buie.B = t.B;
+    p.buie.C = t.C;
+  } else if (sunshape != qm::kSunshapePillbox) {
+    invalid("sunshape must be 0 (Buie) or 1 (pillbox)");
+  }
+  cuda_check(qm::launch_pool(p, 0), "pool kernel");
+  cuda_check(cudaDeviceSynchronize(), "pool kernel");
+}
+
+qmcrt_scene* checked(qmcrt_scene* s) {
+  if (!s) invalid("scene is NULL");
+  if (s->device < 0) throw ApiError(QMCRT_ERR_STATE, "scene was loaded host-only (device -1); it cannot trace");
+  return s;
+}
+
+void check_heliostat(const qmcrt_scene* s, int id) {
+  // QuasiMonteCarloRayTracer::checkValidHeliostatIndex (QuasiMonteCarloRayTracer.cpp:96-127).
+  int n = (int)s->model.heliostats.size();
+  if (id < 0 || id >= n)
+    invalid("The ray tracing heliostat index " + std::to_string(id) +
+            " is invalid. The heliostat index should between 0 and " + std::to_string(n) + ".");
+}
+
+void ensure_stage(qmcrt_scene* s, size_t n) {
+  if (s->stage_done) cuda_check(cudaEventSynchronize(s->stage_done), "cudaEventSynchronize");
+  if (n <= s->stage_cap) return;
+  if (s->h_stage) cudaFreeHost(s->h_stage);
+  if (s->h_prefix) cudaFreeHost(s->h_prefix);
+  s->h_stage = nullptr;
+  s->h_prefix = nullptr;
+  size_t cap = std::max<size_t>(n, 64);
+  cuda_check(cudaMallocHost((void**)&s->h_stage, cap * sizeof(DevTask)), "cudaMallocHost");
+  cuda_check(cudaMallocHost((void**)&s->h_prefix, (cap + 1) * sizeof(long long)), "cudaMallocHost");
+  s->d_tasks.alloc(cap * sizeof(DevTask));
+  s->d_prefix.alloc((cap + 1) * sizeof(long long));
+  s->stage_cap = cap;
+  s->cache_valid = false;
+}
+
+qm::TraceParams base_params(qmcrt_scene* s) {
+  qm::TraceParams p{};
+  p.grids = s->d_grids.as<DevGrid>();
+  p.receivers = s->d_receivers.as<DevReceiver>();
+  p.samples = s->d_samples.as<float4>();
+  p.perturbations = s->d_perturb.as<float4>();
+  p.pool_size = s->pool_size;
+  p.light_begin = s->light_begin;
+  p.light_end = s->light_end;
+  p.sun = s->sun;
+  p.power = s->d_power.as<double>();
+  p.diag = s->d_diag.as<unsigned long long>();
+  return p;
+}
+
+cudaError_t run_trace(qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st) {
+  return s->exact ? qm::launch_trace_exact(p, record, st) : qm::launch_trace_fast(p, record, st);
+}
+
+void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
+  if (n < 0 || (n > 0 && !ids)) invalid("heliostat list is invalid");
+  for (int i = 0; i < n; ++i) check_heliostat(s, ids[i]);
+  if (n == 0) return;
+  DeviceGuard guard(s->device);
+  bool same = s->cache_valid && (int)s->cached_ids.size() == n && std::equal(ids, ids + n, s->cached_ids.begin());
+  long long total = 0;
+  if (!same) {
+    ensure_stage(s, (size_t)n);
+    s->h_prefix[0] = 0;
+    for (int i = 0; i < n; ++i) {
+      s->h_stage[i] = s->templates[ids[i]];
+      s->h_prefix[i + 1] = s->h_prefix[i] + s->templates[ids[i]].num_facets;
+    }
+    cuda_check(cudaMemcpyAsync(s->d_tasks.p, s->h_stage, n * sizeof(DevTask), cudaMemcpyHostToDevice, stream),
+               "task upload");
+    cuda_check(cudaMemcpyAsync(s->d_prefix.p, s->h_prefix, (n + 1) * sizeof(long long), cudaMemcpyHostToDevice, stream),
+               "task upload");
+    if (!s->stage_done) cuda_check(cudaEventCreateWithFlags(&s->stage_done, cudaEventDisableTiming), "cudaEventCreate");
+    cuda_check(cudaEventRecord(s->stage_done, stream), "cudaEventRecord");
+    s->cached_ids.assign(ids, ids + n);
+    s->cache_valid = true;
+  }
+  for (int i = 0; i < n; ++i) total += s->templates[ids[i]].num_facets;
+  qm::TraceParams p = base_params(s);
+  p.tasks = s->d_tasks.as<DevTask>();
+  p.facet_prefix = s->d_prefix.as<long long>();
+  p.num_tasks = n;
+  p.total_facets = total;
+  cuda_check(run_trace(s, p, false, stream), "trace kernel");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* qmcrt_last_error(void) { return g_last_error.c_str(); }
+
+int qmcrt_version(void) { return 1; }
+
+int qmcrt_scene_load(const char* scene_path, const char* config_path, int device, unsigned seed, qmcrt_scene** out) {
+  return guarded([&] {
+    if (!out) invalid("out is NULL");
+    *out = nullptr;
+    if (!scene_path || !config_path) invalid("scene and configuration paths are required");
+    if (device >= 0) {
+      int ndev = 0;
+      cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
+      if (device >= ndev) invalid("device index out of range");
+    }
+    std::unique_ptr<qmcrt_scene> s(new qmcrt_scene());
+    s->device = device;
+    s->seed = seed;
+    std::string err;
+    int fields = qm::read_config_file(config_path, s->model.config, err);
+    if (fields < 0) throw ApiError(QMCRT_ERR_IO, err);
+    qm::SceneConfig cfg = s->model.config;
+    if (!qm::read_scene_file(scene_path, s->model, err)) throw ApiError(QMCRT_ERR_IO, err);
+    s->model.config = cfg;
+    s->model.config_fields = fields;
+    if (!qm::process_scene(s->model, err)) throw ApiError(QMCRT_ERR_INVALID, err);
+    if (device < 0) {
+      // Host-only scene: the processed model without device buffers, for
+      // inspecting geometry on a machine without a GPU.
+      const auto& c = s->model.config;
+      s->pool_size = c.num_sunshape_groups * c.num_per_sunshape_group;
+      for (const auto& h : s->model.heliostats) s->total_facets += h.num_facets;
+      *out = s.release();
+      return;
+    }
+    DeviceGuard guard(device);
+    build_device_scene(s.get());
+    generate_pool(s.get(), seed, qm::kSunshapeBuie, 0.00465f);
+    generate_offsets(s.get(), seed);
+    *out = s.release();
+  });
+}
+
+void qmcrt_scene_free(qmcrt_scene* s) { delete s; }
+
+int qmcrt_scene_get_info(const qmcrt_scene* s, qmcrt_scene_info* info) {
+  return guarded([&] {
+    if (!s || !info) invalid("scene or info is NULL");
+    const auto& m = s->model;
+    const auto& c = m.config;
+    std::memset(info, 0, sizeof(*info));
+    info->num_receivers = (int)m.receivers.size();
+    info->num_grids = (int)m.grids.size();
+    info->num_heliostats = (int)m.heliostats.size();
+    info->num_sunshape_groups = c.num_sunshape_groups;
+    info->num_per_sunshape_group = c.num_per_sunshape_group;
+    info->pool_size = s->pool_size;
+    info->inverse_transform_sampling_groups = c.inverse_transform_sampling_groups;
+    info->config_fields = m.config_fields;
+    info->sun_dir[0] = c.sun_dir.x;
+    info->sun_dir[1] = c.sun_dir.y;
+    info->sun_dir[2] = c.sun_dir.z;
+    info->dni = c.dni;
+    info->csr = c.csr;
+    info->receiver_pixel_length = c.receiver_pixel_length;
+    info->helio_disturb_std = c.helio_disturb_std;
+    info->helio_pixel_length = c.helio_pixel_length;
+    info->helio_reflected_rate = c.helio_reflected_rate;
+    info->ground_length = m.ground_length;
+    info->ground_width = m.ground_width;
+    info->total_facets = s->total_facets;
+  });
+}
+
+int qmcrt_receiver_get(const qmcrt_scene* s, int id, int* type, int* width, int* height, float* pixel_length,
+                       float* vertices12, float* normal3, float* focus3) {
+  return guarded([&] {
+    if (!s) invalid("scene is NULL");
+    if (id < 0 || id >= (int)s->model.receivers.size()) invalid("receiver index out of range");
+    const auto& r = s->model.receivers[id];
+    if (type) *type = r.type;
+    if (width) *width = r.resolution.x;
+    if (height) *height = r.resolution.y;
+    if (pixel_length) *pixel_length = r.pixel_length;
+    if (vertices12)
+      for (int k = 0; k < 4; ++k) {
+        vertices12[3 * k] = r.vertex[k].x;
+        vertices12[3 * k + 1] = r.vertex[k].y;
+        vertices12[3 * k + 2] = r.vertex[k].z;
+      }
+    if (normal3) {
+      normal3[0] = r.normal.x;
+      normal3[1] = r.normal.y;
+      normal3[2] = r.normal.z;
+    }
+    if (focus3) {
+      focus3[0] = r.focus.x;
+      focus3[1] = r.focus.y;
+      focus3[2] = r.focus.z;
+    }
+  });
+}
+
+int qmcrt_heliostat_get(const qmcrt_scene* s, int id, int* type, int* grid, int* num_facets, int* num_sub,
+                        int* sub_begin, float* pos3, float* size3, float* normal3, float* focus_length) {
+  return guarded([&] {
+    if (!s) invalid("scene is NULL");
+    check_heliostat(s, id);
+    const auto& h = s->model.heliostats[id];
+    if (type) *type = h.type;
+    if (grid) *grid = h.grid;
+    if (num_facets) *num_facets = h.num_facets;
+    if (num_sub) *num_sub = h.num_sub;
+    if (sub_begin) *sub_begin = h.sub_begin;
+    if (pos3) pos3[0] = h.pos.x, pos3[1] = h.pos.y, pos3[2] = h.pos.z;
+    if (size3) size3[0] = h.size.x, size3[1] = h.size.y, size3[2] = h.size.z;
+    if (normal3) normal3[0] = h.normal.x, normal3[1] = h.normal.y, normal3[2] = h.normal.z;
+    if (focus_length) *focus_length = h.focus_length;
+  });
+}
+
+int qmcrt_grid_get(const qmcrt_scene* s, int id, int* cells3, int* num_sub, int* nnz, int* receiver, int* start,
+                   int* count) {
+  return guarded([&] {
+    if (!s) invalid("scene is NULL");
+    if (id < 0 || id >= (int)s->model.grids.size()) invalid("grid index out of range");
+    const auto& g = s->model.grids[id];
+    if (cells3) cells3[0] = g.cells.x, cells3[1] = g.cells.y, cells3[2] = g.cells.z;
+    if (num_sub) *num_sub = g.num_subheliostats;
+    if (nnz) *nnz = (int)g.cell_match.size();
+    if (receiver) *receiver = g.receiver;
+    if (start) *start = g.start_heliostat;
+    if (count) *count = g.num_heliostats;
+  });
+}
+
+int qmcrt_grid_csr(const qmcrt_scene* s, int id, int* index, int* match) {
+  return guarded([&] {
+    if (!s) invalid("scene is NULL");
+    if (id < 0 || id >= (int)s->model.grids.size()) invalid("grid index out of range");
+    const auto& g = s->model.grids[id];
+    if (index) std::copy(g.cell_index.begin(), g.cell_index.end(), index);
+    if (match) std::copy(g.cell_match.begin(), g.cell_match.end(), match);
+  });
+}
+
+int qmcrt_grid_vertices(const qmcrt_scene* s, int id, float* xyz) {
+  return guarded([&] {
+    if (!s || !xyz) invalid("scene or output is NULL");
+    if (id < 0 || id >= (int)s->model.grids.size()) invalid("grid index out of range");
+    const auto& g = s->model.grids[id];
+    for (size_t i = 0; i < g.sub_vertices.size(); ++i) {
+      xyz[3 * i] = g.sub_vertices[i].x;
+      xyz[3 * i + 1] = g.sub_vertices[i].y;
+      xyz[3 * i + 2] = g.sub_vertices[i].z;
+    }
+  });
+}
+
+int qmcrt_heliostat_facets(qmcrt_scene* s, int id, float* origins, float* normals) {
+  return guarded([&] {
+    checked(s);
+    check_heliostat(s, id);
+    if (!origins || !normals) invalid("output is NULL");
+    DeviceGuard guard(s->device);
+    const DevTask& t = s->templates[id];
+    DBuf o, n;
+    o.alloc(std::max<size_t>(t.num_facets, 1) * sizeof(float3));
+    n.alloc(std::max<size_t>(t.num_facets, 1) * sizeof(float3));
+    cudaError_t e = s->exact ? qm::launch_facets_exact(t, o.as<float3>(), n.as<float3>(), 0)
+                             : qm::launch_facets_fast(t, o.as<float3>(), n.as<float3>(), 0);
+    cuda_check(e, "facets kernel");
+    cuda_check(cudaMemcpy(origins, o.p, (size_t)t.num_facets * sizeof(float3), cudaMemcpyDeviceToHost), "readback");
+    cuda_check(cudaMemcpy(normals, n.p, (size_t)t.num_facets * sizeof(float3), cudaMemcpyDeviceToHost), "readback");
+  });
+}
+
+int qmcrt_set_sample_pool(qmcrt_scene* s, const float* dirs, const float* perturb, int groups, int per_group,
+                          int on_device) {
+  return guarded([&] {
+    checked(s);
+    if (!dirs || !perturb) invalid("pool pointers are NULL");
+    if (groups <= 0 || per_group <= 0 || (long long)groups * per_group != s->pool_size ||
+        per_group != s->model.config.num_per_sunshape_group)
+      invalid("pool shape must match the configuration's groups x lights-per-group");
+    DeviceGuard guard(s->device);
+    const int n = s->pool_size;
+    DBuf tmp;
+    tmp.alloc((size_t)n * 3 * sizeof(float));
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    cuda_check(cudaMemcpy(tmp.p, dirs, (size_t)n * 3 * sizeof(float), kind), "pool upload");
+    cuda_check(qm::launch_xyz_to_float4(tmp.as<float>(), s->d_samples.as<float4>(), n, 0), "pool convert");
+    cuda_check(cudaMemcpy(tmp.p, perturb, (size_t)n * 3 * sizeof(float), kind), "pool upload");
+    cuda_check(qm::launch_xyz_to_float4(tmp.as<float>(), s->d_perturb.as<float4>(), n, 0), "pool convert");
+    cuda_check(cudaDeviceSynchronize(), "pool convert");
+  });
+}
+
+int qmcrt_generate_sample_pool(qmcrt_scene* s, unsigned seed, int sunshape, float half_angle) {
+  return guarded([&] {
+    checked(s);
+    if (sunshape == qm::kSunshapePillbox && !(half_angle > 0.0f && half_angle < 1.0f))
+      invalid("pillbox half-angle must be in (0, 1) radians");
+    DeviceGuard guard(s->device);
+    generate_pool(s, seed, sunshape, half_angle);
+  });
+}
+
+int qmcrt_get_sample_pool(qmcrt_scene* s, float* dirs, float* perturb) {
+  return guarded([&] {
+    checked(s);
+    DeviceGuard guard(s->device);
+    std::vector<float4> tmp(s->pool_size);
+    if (dirs) {
+      cuda_check(cudaMemcpy(tmp.data(), s->d_samples.p, tmp.size() * sizeof(float4), cudaMemcpyDeviceToHost), "readback");
+      for (size_t i = 0; i < tmp.size(); ++i) dirs[3 * i] = tmp[i].x, dirs[3 * i + 1] = tmp[i].y, dirs[3 * i + 2] = tmp[i].z;
+    }
+    if (perturb) {
+      cuda_check(cudaMemcpy(tmp.data(), s->d_perturb.p, tmp.size() * sizeof(float4), cudaMemcpyDeviceToHost), "readback");
+      for (size_t i = 0; i < tmp.size(); ++i)
+        perturb[3 * i] = tmp[i].x, perturb[3 * i + 1] = tmp[i].y, perturb[3 * i + 2] = tmp[i].z;
+    }
+  });
+}
+
+int qmcrt_set_facet_offsets(qmcrt_scene* s, int id, const int* offsets, int n) {
+  return guarded([&] {
+    checked(s);
+    check_heliostat(s, id);
+    const int nf = s->model.heliostats[id].num_facets;
+    if (!offsets || (n != nf && n != nf + 1)) invalid("offsets must hold num_facets or num_facets + 1 entries");
+    std::vector<int> v(offsets, offsets + n);
+    if (n == nf) v.push_back(nf > 0 ? v[0] : 0);
+    for (int x : v)
+      if (x < 0 || x >= s->pool_size) invalid("facet offsets must lie in [0, pool_size)");
+    DeviceGuard guard(s->device);
+    cuda_check(cudaMemcpy(s->d_offsets.as<int>() + s->offset_base[id], v.data(), v.size() * sizeof(int),
+                          cudaMemcpyHostToDevice),
+               "offsets upload");
+  });
+}
+
+int qmcrt_get_facet_offsets(qmcrt_scene* s, int id, int* offsets, int n) {
+  return guarded([&] {
+    checked(s);
+    check_heliostat(s, id);
+    const int nf = s->model.heliostats[id].num_facets;
+    if (!offsets || n < 0 || n > nf + 1) invalid("offsets buffer size out of range");
+    DeviceGuard guard(s->device);
+    cuda_check(cudaMemcpy(offsets, s->d_offsets.as<int>() + s->offset_base[id], (size_t)n * sizeof(int),
+                          cudaMemcpyDeviceToHost),
+               "offsets readback");
+  });
+}
+
+int qmcrt_generate_facet_offsets(qmcrt_scene* s, unsigned seed) {
+  return guarded([&] {
+    checked(s);
+    DeviceGuard guard(s->device);
+    generate_offsets(s, seed);
+  });
+}
+
+int qmcrt_set_math_mode(qmcrt_scene* s, int exact) {
+  return guarded([&] { checked(s)->exact = exact ? 1 : 0; });
+}
+
+int qmcrt_set_light_range(qmcrt_scene* s, int begin, int end) {
+  return guarded([&] {
+    checked(s);
+    if (begin < 0 || end < begin || end > s->model.config.num_per_sunshape_group)
+      invalid("light range must satisfy 0 <= begin <= end <= num_per_sunshape_group");
+    s->light_begin = begin;
+    s->light_end = end;
+  });
+}
+
+int qmcrt_trace_heliostat(qmcrt_scene* s, int id, void* stream) {
+  return guarded([&] { trace_ids(checked(s), &id, 1, static_cast<cudaStream_t>(stream)); });
+}
+
+int qmcrt_trace_heliostats(qmcrt_scene* s, const int* ids, int n, void* stream) {
+  return guarded([&] { trace_ids(checked(s), ids, n, static_cast<cudaStream_t>(stream)); });
+}
+
+int qmcrt_receiver_image(qmcrt_scene* s, int id, float* out, int* width, int* height) {
+  return guarded([&] {
+    checked(s);
+    if (id < 0 || id >= (int)s->model.receivers.size()) invalid("receiver index out of range");
+    const auto& r = s->model.receivers[id];
+    if (width) *width = r.resolution.x;
+    if (height) *height = r.resolution.y;
+    if (out) {
+      DeviceGuard guard(s->device);
+      cuda_check(cudaDeviceSynchronize(), "synchronise");
+      cuda_check(cudaMemcpy(out, s->images[id]->p, (size_t)r.resolution.x * r.resolution.y * sizeof(float),
+                            cudaMemcpyDeviceToHost),
+                 "image readback");
+    }
+  });
+}
+
+int qmcrt_receiver_device_image(qmcrt_scene* s, int id, float** dptr, int* width, int* height) {
+  return guarded([&] {
+    checked(s);
+    if (id < 0 || id >= (int)s->model.receivers.size()) invalid("receiver index out of range");
+    const auto& r = s->model.receivers[id];
+    if (dptr) *dptr = s->images[id]->as<float>();
+    if (width) *width = r.resolution.x;
+    if (height) *height = r.resolution.y;
+  });
+}
+
+int qmcrt_receiver_clear(qmcrt_scene* s, int id, void* stream) {
+  return guarded([&] {
+    checked(s);
+    if (id < 0 || id >= (int)s->model.receivers.size()) invalid("receiver index out of range");
+    DeviceGuard guard(s->device);
+    cuda_check(cudaMemsetAsync(s->images[id]->p, 0, s->images[id]->bytes, static_cast<cudaStream_t>(stream)),
+               "image clear");
+  });
+}
+
+int qmcrt_power_fp64(qmcrt_scene* s, double* per, double* total) {
+  return guarded([&] {
+    checked(s);
+    DeviceGuard guard(s->device);
+    std::vector<double> v(s->model.heliostats.size());
+    cuda_check(cudaDeviceSynchronize(), "synchronise");
+    if (!v.empty())
+      cuda_check(cudaMemcpy(v.data(), s->d_power.p, v.size() * sizeof(double), cudaMemcpyDeviceToHost), "readback");
+    if (per) std::copy(v.begin(), v.end(), per);
+    if (total) {
+      // Neumaier-compensated sum of the per-heliostat totals.
+      double sum = 0.0, comp = 0.0;
+      for (double x : v) {
+        double t = sum + x;
+        comp += (std::fabs(sum) >= std::fabs(x)) ? (sum - t) + x : (x - t) + sum;
+        sum = t;
+      }
+      *total = sum + comp;
+    }
+  });
+}
+
+int qmcrt_power_clear(qmcrt_scene* s) {
+  return guarded([&] {
+    checked(s);
+    DeviceGuard guard(s->device);
+    cuda_check(cudaDeviceSynchronize(), "synchronise");
+    cuda_check(cudaMemset(s->d_power.p, 0, s->d_power.bytes), "clear");
+    cuda_check(cudaMemset(s->d_diag.p, 0, s->d_diag.bytes), "clear");
+  });
+}
+
+int qmcrt_diagnostics(qmcrt_scene* s, unsigned long long* out4) {
+  return guarded([&] {
+    checked(s);
+    if (!out4) invalid("output is NULL");
+    DeviceGuard guard(s->device);
+    cuda_check(cudaDeviceSynchronize(), "synchronise");
+    cuda_check(cudaMemcpy(out4, s->d_diag.p, qm::kDiagSlots * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+               "readback");
+  });
+}
+
+int qmcrt_debug_hit_records(qmcrt_scene* s, int id, int fb, int fe, int lb, int le, int* codes) {
+  return guarded([&] {
+    checked(s);
+    check_heliostat(s, id);
+    const int nf = s->model.heliostats[id].num_facets;
+    if (fb < 0 || fe < fb || fe > nf) invalid("facet range out of bounds");
+    if (lb < 0 || le < lb || le > s->model.config.num_per_sunshape_group) invalid("light range out of bounds");
+    if (!codes) invalid("output is NULL");
+    const size_t count = (size_t)(fe - fb) * (le - lb);
+    if (count == 0) return;
+    DeviceGuard guard(s->device);
+    // Scratch receivers, power and counters so the scene's state is untouched.
+    std::vector<DevReceiver> recv = s->receivers;
+    size_t maxpix = 1;
+    for (auto& r : recv) maxpix = std::max(maxpix, (size_t)r.resolution.x * r.resolution.y);
+    DBuf img, dr, rec, pw, dg, task, prefix;
+    img.alloc(maxpix * sizeof(float));
+    for (auto& r : recv) r.image = img.as<float>();
+    upload(dr, recv);
+    rec.alloc(count * sizeof(int32_t));
+    pw.alloc(s->model.heliostats.size() * sizeof(double) + 8);
+    dg.alloc(qm::kDiagSlots * sizeof(unsigned long long));
+    std::vector<DevTask> one{s->templates[id]};
+    upload(task, one);
+    qm::TraceParams p = base_params(s);
+    p.receivers = dr.as<DevReceiver>();
+    p.tasks = task.as<DevTask>();
+    p.num_tasks = 1;
+    p.power = pw.as<double>();
+    p.diag = dg.as<unsigned long long>();
+    p.light_begin = lb;
+    p.light_end = le;
+    p.records = rec.as<int32_t>();
+    p.record_task = 0;
+    p.record_facet_begin = fb;
+    p.record_facet_end = fe;
+    cuda_check(run_trace(s, p, true, 0), "record kernel");
+    cuda_check(cudaMemcpy(codes, rec.p, count * sizeof(int32_t), cudaMemcpyDeviceToHost), "readback");
+  });
+}
+
+int qmcrt_smooth(float* d_img, int width, int height, int radius, float ratio, void* stream) {
+  return guarded([&] {
+    if (!d_img) invalid("image is NULL");
+    if (width <= 0 || height <= 0) invalid("image size must be positive");
+    if (radius < 0 || radius > 64) invalid("radius must be in [0, 64]");
+    if (!(ratio >= 0.0f && ratio < 0.5f)) invalid("trim ratio must be in [0, 0.5)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t bytes = (size_t)width * height * sizeof(float);
+    void* copy = nullptr;
+    cuda_check(cudaMallocAsync(&copy, bytes, st), "cudaMallocAsync");
+    cudaError_t e = cudaMemcpyAsync(copy, d_img, bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = qm::launch_trimmed_mean(static_cast<float*>(copy), d_img, width, height, radius, ratio, st);
+    cudaFreeAsync(copy, st);
+    cuda_check(e, "trimmed mean");
+  });
+}
+
+int qmcrt_load_tasks(const qmcrt_scene* s, const char* path, int* hs, int* nh, int capacity, int* rs, int* nr,
+                     int* status) {
+  return guarded([&] {
+    if (!s || !path) invalid("scene or path is NULL");
+    std::vector<int> h, r;
+    std::string err;
+    int st = qm::read_task_file(path, s->model, h, r, err);
+    if (st < 0) throw ApiError(QMCRT_ERR_IO, err);
+    if ((int)h.size() > capacity || (int)r.size() > capacity) invalid("task buffers are too small");
+    if (hs) std::copy(h.begin(), h.end(), hs);
+    if (rs) std::copy(r.begin(), r.end(), rs);
+    if (nh) *nh = (int)h.size();
+    if (nr) *nr = (int)r.size();
+    if (status) *status = st;
+  });
+}
+
+int qmcrt_save_text(const char* path, int height, int width, const float* data, int precision, float* max_value) {
+  return guarded([&] {
+    if (!path || !data || height < 0 || width < 0 || precision < 0 || precision > 30) invalid("bad arguments");
+    std::string err;
+    bool ok = false;
+    float m = qm::save_text_image(path, height, width, data, precision, err, &ok);
+    if (!ok) throw ApiError(QMCRT_ERR_IO, err);
+    if (max_value) *max_value = m;
+  });
+}
+
+}  // extern "C"

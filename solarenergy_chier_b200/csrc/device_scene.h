@@ -1,0 +1,89 @@
+// Plain-old-data views of a processed scene, as the sm_100a kernels read them.
+// Built on the host by capi.cpp from the float32 scene model (scene.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace qm {
+
+// One RectangleGrid (Scene/DataStructure/Grid/RectangleGrid.cuh:13-52) in
+// traversal form.
+struct DevGrid {
+  float3 pos;
+  float3 interval;
+  int3 cells;
+  int max_steps;        // DDA step bound: cells.x + cells.y + cells.z + 2
+  const int* hindex;    // heliostat-level CSR offsets, cells + 1 entries
+  const int* hmatch;    // grid-local heliostat ids per cell
+  const float4* bound;  // 4 float4 per grid-local heliostat: centre, then (axis_k, half extent_k)
+  const int2* hsub;     // (first sub-heliostat id, sub-heliostat count) per grid-local heliostat
+  const float4* subv;   // 3 float4 per sub-heliostat: A.xyz AB.x | AB.yz AC.xy | AC.z
+};
+
+struct DevReceiver {
+  int type;             // 0 rectangle, 1 cylinder
+  int2 resolution;      // x = columns, y = rows
+  float* image;         // resolution.x * resolution.y floats, row-major by row
+  float3 a, ab, ac;     // rectangle: vertex 0, v1 - v0, v3 - v0
+  float3 pos, size;     // cylinder: centre, (radius, height, -)
+};
+
+// One heliostat to trace (a HeliostatArgument plus the per-heliostat
+// constants of QuasiMonteCarloRayTracer::rayTracing).
+struct DevTask {
+  int type;             // 0 flat, 1 focus-flat
+  int grid;
+  int receiver;
+  int own;              // grid-local heliostat id, skipped by the DDA
+  int num_facets;
+  int power_slot;
+  int2 row_col;
+  int2 sub_row_col;
+  float pixel_length;
+  float factor;
+  float2 gap;
+  float2 sub_length;    // x along z (rows), y along x (columns)
+  float3 size;
+  float3 pos;
+  float3 normal;
+  float3 fu, fn, fv;    // frame of the heliostat normal (plain or flipped variant)
+  int frame_identity;
+  const float3* local_centers;  // focus-flat: per sub-heliostat
+  const float3* local_normals;
+  const int* offsets;   // num_facets + 1 pool offsets
+};
+
+struct SunFrame {
+  float3 u, n, v;
+  int identity;
+};
+
+// Per-ray outcome codes written by the hit-record variant; a hit stores its
+// pixel index (>= 0).
+enum RayCode : int32_t { kShadowed = -1, kBlocked = -2, kMissed = -3, kNotTraced = -4 };
+
+// Diagnostic counters (unsigned long long each).
+enum DiagSlot { kDiagClamped = 0, kDiagDdaCap = 1, kDiagSlots = 4 };
+
+struct TraceParams {
+  const DevGrid* grids;
+  const DevReceiver* receivers;
+  const DevTask* tasks;
+  const long long* facet_prefix;  // num_tasks + 1
+  int num_tasks;
+  long long total_facets;
+  const float4* samples;          // sun-shape pool, P entries (xyz used)
+  const float4* perturbations;    // slope-error pool, P entries
+  int pool_size;
+  int light_begin, light_end;     // light indexes traced per facet
+  SunFrame sun;                   // frame of -sun_dir
+  double* power;                  // FP64 per-slot power accumulators
+  unsigned long long* diag;
+  // hit-record variant only
+  int32_t* records;
+  int record_task;
+  int record_facet_begin, record_facet_end;
+};
+
+}  // namespace qm

@@ -1,0 +1,49 @@
+// Sample-pool and facet-offset generation (device) and the Buie sun-shape
+// table (host).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace qm {
+
+enum Sunshape : int { kSunshapeBuie = 0, kSunshapePillbox = 1 };
+
+// Device view of the reference's Buie inverse-CDF table.
+struct BuieTable {
+  const float2* cdf;  // n + 1 (theta mrad, cumulative) pairs
+  const float* k;     // n slopes
+  int n;
+  float less_465;     // integral of the core, 0..4.65 mrad
+  float gamma, A, B, C;
+};
+
+// Host copy: SceneProcessor::set_samplelights parameters
+// (Scene/SceneProcessor.cu:196-240 with parameters_generate, :23-44), float
+// arithmetic in the reference's order.
+struct BuieHost {
+  std::vector<float2> cdf;
+  std::vector<float> k;
+  float less_465 = 0.f, gamma = 0.f, A = 0.f, B = 0.f, C = 0.f, kappa = 0.f;
+};
+BuieHost build_buie_table(float csr, int num_group);
+
+struct PoolParams {
+  float4* samples;
+  float4* perturbations;
+  int pool_size;
+  int sunshape;
+  float half_angle;   // pillbox half-angle, radians
+  float sigma;        // slope-error standard deviation, radians
+  uint32_t seed_sun;
+  uint32_t seed_slope;
+  BuieTable buie;
+};
+
+cudaError_t launch_pool(const PoolParams& p, cudaStream_t stream);
+cudaError_t launch_offsets(int* out, long long count, uint32_t seed, int heliostat, int pool, cudaStream_t stream);
+cudaError_t launch_xyz_to_float4(const float* xyz, float4* out, int n, cudaStream_t stream);
+
+}  // namespace qm

@@ -1,0 +1,322 @@
+// Quasi-Monte-Carlo heliostat tracer for sm_100a.
+//
+// One warp owns one micro-facet; its 32 lanes take consecutive light indexes
+// (the reference's thread order in map_raytracing, so the 32 rays of a warp
+// share an origin and nearly share a direction and their grid walks stay
+// together).  A launch covers every facet of every traced heliostat: there
+// is no per-heliostat launch, allocation or synchronisation.
+//
+// Per ray (QuasiMonteCarloRayTracing/RectangleReceiverRectangleGridRayTracing.cu:6-41
+// and CylinderReceiverRectangleGridRayTracing.cu:6-40):
+//   sun sample -> world direction, shadow walk toward the sun, slope-error
+//   normal, reflection, block walk, receiver hit, energy, flux deposit.
+// The walk is the reference's 3D-DDA (QuasiMonteCarloRayTracing/Grid/rectGridDDA.cu:31-119)
+// step for step, including its 1e-5 tie rules and truncating start cell.
+// Inside a cell each heliostat is first tested against a padded bounding
+// box in its own frame; only boxes the ray enters have their sub-heliostat
+// parallelograms tested.  The box is conservative (padding far above float
+// rounding) so the any-hit answer is unchanged.
+//
+// This file is compiled twice: QM_TRACE_VARIANT=exact with -fmad=false (each
+// float operation rounds as in the CPU oracle) and QM_TRACE_VARIANT=fast with
+// FMA contraction (production).
+#include <climits>
+
+#include "device_scene.h"
+#include "tracer.h"
+#include "vecmath.h"
+
+#ifndef QM_TRACE_VARIANT
+#define QM_TRACE_VARIANT fast
+#endif
+#define QM_CAT2(a, b) a##_##b
+#define QM_CAT(a, b) QM_CAT2(a, b)
+#define QM_SYM(name) QM_CAT(name, QM_TRACE_VARIANT)
+
+namespace qm {
+namespace {
+
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+
+// rectGridDDA::absDivide / calTMax / equal / less (rectGridDDA.cuh:15-32).
+__device__ __forceinline__ float abs_divide(float den, float num) {
+  if ((double)num <= kEps && (double)num >= -kEps) return (float)INT_MAX;
+  return fabsf(den / num);
+}
+__device__ __forceinline__ float cal_tmax(float dir, float interval, int index, float pos) {
+  return fabsf(float(index + (dir >= 0)) * interval - pos);
+}
+__device__ __forceinline__ bool eq_eps(float a, float b) {
+  return ((double)a < (double)b + kEps) && ((double)a > (double)b - kEps);
+}
+__device__ __forceinline__ bool lt_eps(float a, float b) { return (double)a < (double)b - kEps; }
+
+// Conservative slab test against one heliostat's padded box.
+__device__ __forceinline__ void slab(float3 r, float3 d, float4 ax, float& tn, float& tf) {
+  float ol = r.x * ax.x + r.y * ax.y + r.z * ax.z;
+  float dl = d.x * ax.x + d.y * ax.y + d.z * ax.z;
+  float inv = __fdividef(1.0f, dl);
+  float t0 = (-ax.w - ol) * inv;
+  float t1 = (ax.w - ol) * inv;
+  tn = fmaxf(tn, fminf(t0, t1));
+  tf = fminf(tf, fmaxf(t0, t1));
+}
+
+__device__ __forceinline__ bool box_hit(const float4* b, float3 o, float3 d) {
+  float4 c = __ldg(b);
+  float3 r = make_float3(o.x - c.x, o.y - c.y, o.z - c.z);
+  float tn = -3.0e38f, tf = 3.0e38f;
+  slab(r, d, __ldg(b + 1), tn, tf);
+  slab(r, d, __ldg(b + 2), tn, tf);
+  slab(r, d, __ldg(b + 3), tn, tf);
+  return tn <= tf && tf >= -1.0f;
+}
+
+__device__ __forceinline__ bool sub_hit(const float4* sv, float3 o, float3 d) {
+  float4 p0 = __ldg(sv), p1 = __ldg(sv + 1), p2 = __ldg(sv + 2);
+  float t, u, v;
+  return ray_parallelogram(o, d, make_float3(p0.x, p0.y, p0.z), make_float3(p0.w, p1.x, p1.y),
+                           make_float3(p1.z, p1.w, p2.x), t, u, v);
+}
+
+// rectGridDDA::intersect over one cell (rectGridDDA.cu:7-25).
+__device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, float3 o, float3 d) {
+  int b = __ldg(g.hindex + cell), e = __ldg(g.hindex + cell + 1);
+  for (int k = b; k < e; ++k) {
+    int h = __ldg(g.hmatch + k);
+    if (h == own) continue;
+    int2 sr = __ldg(g.hsub + h);
+    if (sr.y > 1 && !box_hit(g.bound + 4 * h, o, d)) continue;
+    for (int s = sr.x; s < sr.x + sr.y; ++s)
+      if (sub_hit(g.subv + 3 * s, o, d)) return true;
+  }
+  return false;
+}
+
+// rectGridDDA::collision (rectGridDDA.cu:31-119).  The reference loops until
+// the walk leaves the grid; a walk that stops advancing (an exact tie the
+// reference never leaves) or exceeds cells.x+cells.y+cells.z+2 steps ends
+// here with "no hit" and a diagnostic count instead.
+__device__ bool collide(const DevGrid& g, int own, float3 o, float3 d, unsigned& flags) {
+  float3 rel = make_float3(o.x - g.pos.x, o.y - g.pos.y, o.z - g.pos.z);
+  int3 c = trunc3(cdiv(rel, g.interval));
+  int3 st = make_int3(d.x >= 0 ? 1 : -1, d.y >= 0 ? 1 : -1, d.z >= 0 ? 1 : -1);
+  float3 tm, td;
+  tm.x = abs_divide(cal_tmax(d.x, g.interval.x, c.x, rel.x), d.x);
+  tm.y = abs_divide(cal_tmax(d.y, g.interval.y, c.y, rel.y), d.y);
+  tm.z = abs_divide(cal_tmax(d.z, g.interval.z, c.z, rel.z), d.z);
+  td.x = abs_divide(g.interval.x, d.x);
+  td.y = abs_divide(g.interval.y, d.y);
+  td.z = abs_divide(g.interval.z, d.z);
+  for (int it = 0; it < g.max_steps; ++it) {
+    if (c.x < 0 || c.x >= g.cells.x || c.y < 0 || c.y >= g.cells.y || c.z < 0 || c.z >= g.cells.z) return false;
+    int cell = c.x * g.cells.y * g.cells.z + c.y * g.cells.z + c.z;
+    if (cell_hit(g, cell, own, o, d)) return true;
+    bool sx = false, sy = false, sz = false;
+    if (lt_eps(tm.x, tm.y)) {
+      if (lt_eps(tm.x, tm.z) || eq_eps(tm.x, tm.z)) { c.x += st.x; sx = true; }
+      if (lt_eps(tm.z, tm.x) || eq_eps(tm.x, tm.z)) { c.z += st.z; sz = true; }
+    } else if (lt_eps(tm.y, tm.x)) {
+      if (lt_eps(tm.y, tm.z) || eq_eps(tm.y, tm.z)) { c.y += st.y; sy = true; }
+      if (lt_eps(tm.z, tm.y) || eq_eps(tm.y, tm.z)) { c.z += st.z; sz = true; }
+    } else {
+      if (lt_eps(tm.x, tm.z) || eq_eps(tm.x, tm.z)) { c.x += st.x; c.y += st.y; sx = sy = true; }
+      if (lt_eps(tm.z, tm.x) || eq_eps(tm.x, tm.z)) { c.z += st.z; sz = true; }
+    }
+    if (!(sx || sy || sz)) {
+      flags |= 2u;
+      return false;
+    }
+    tm.x += sx ? td.x : 0;
+    tm.y += sy ? td.y : 0;
+    tm.z += sz ? td.z : 0;
+  }
+  flags |= 2u;
+  return false;
+}
+
+// CylinderReceiver::GIntersect (Scene/DataStructure/Receiver/CylinderReceiver.cuh:39-89).
+// acos takes its argument clamped to [-1, 1]; the reference prints an error
+// and lets a NaN through when rounding pushes it outside.
+__device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
+  float2 l = make_float2(o.x - r.pos.x, o.z - r.pos.z);
+  if (dot2(l, l) <= r.size.x * r.size.x) return false;
+  float2 ro = make_float2(r.pos.x - o.x, r.pos.z - o.z);
+  float tp = dot2(ro, normalize2(make_float2(d.x, d.z)));
+  float delta = dot2(ro, ro) - tp * tp;
+  float r2 = r.size.x * r.size.x;
+  if ((double)tp < -kEps || delta > r2) return false;
+  float t_plus = delta <= 0.0f ? r.size.x : sqrtf(r2 - delta);
+  t = (tp - t_plus) / length2(make_float2(d.x, d.z));
+  float3 ip = add(mul(d, t), o);
+  u = (ip.y - r.pos.y) / r.size.y + 0.5f;
+  if (u < 0.0f || u > 1.0f) return false;
+  float2 cs = normalize2(make_float2(ip.x - r.pos.x, ip.z - r.pos.z));
+  float cx = fminf(fmaxf(cs.x, -1.0f), 1.0f);
+  v = (float)((double)acosf(cx) / (2 * M_PI));
+  if (cs.y < 0) v = 1 - v;
+  return true;
+}
+
+__device__ __forceinline__ bool receiver_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
+  if (r.type == 0) return ray_parallelogram(o, d, r.a, r.ab, r.ac, t, u, v);
+  return cylinder_hit(r, o, d, t, u, v);
+}
+
+// Micro-facet centre and normal (rectangle_heliostat::map_microhelio_center_and_normal,
+// Scene/DataStructure/Heliostat/RectangleHelio.cu:54-80; focusFlatRectangle_heliostat
+// kernels, FocusFlatRectangleHelio.cu:12-64), evaluated per facet instead of
+// materialised.
+__device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& origin, float3& normal) {
+  Frame hf;
+  hf.u = T.fu;
+  hf.n = T.fn;
+  hf.v = T.fv;
+  hf.identity = T.frame_identity != 0;
+  const int per_row = T.row_col.y * T.sub_row_col.y;
+  int row = f / per_row;
+  int col = f % per_row;
+  if (T.type == 0) {
+    int brow = row / T.sub_row_col.x;
+    int bcol = col / T.sub_row_col.y;
+    float3 c;
+    c.x = col * T.pixel_length + bcol * T.gap.x + T.pixel_length / 2 - T.size.x / 2;
+    c.y = T.size.y / 2;
+    c.z = row * T.pixel_length + brow * T.gap.y + T.pixel_length / 2 - T.size.z / 2;
+    origin = add(to_world(hf, c), T.pos);
+    normal = T.normal;
+  } else {
+    int block = (row / T.sub_row_col.x) * T.row_col.y + col / T.sub_row_col.y;
+    float3 ln = T.local_normals[block];
+    float3 lc = T.local_centers[block];
+    row %= T.sub_row_col.x;
+    col %= T.sub_row_col.y;
+    float3 lp = make_float3((col + 0.5f) * T.pixel_length - T.sub_length.y / 2, 0.0f,
+                            (row + 0.5f) * T.pixel_length - T.sub_length.x / 2);
+    lp = add(rotate_to(lp, ln, true), lc);
+    normal = to_world(hf, ln);
+    origin = add(to_world(hf, lp), T.pos);
+  }
+}
+
+__device__ __forceinline__ int find_task(const long long* prefix, int n, long long w) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(prefix + mid) <= w) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <bool kRecord>
+__global__ void __launch_bounds__(256) trace_kernel(TraceParams p) {
+  const int lane = threadIdx.x & 31;
+  const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int t, f;
+  if (kRecord) {
+    if (warp >= (long long)(p.record_facet_end - p.record_facet_begin)) return;
+    t = p.record_task;
+    f = p.record_facet_begin + (int)warp;
+  } else {
+    if (warp >= p.total_facets) return;
+    t = find_task(p.facet_prefix, p.num_tasks, warp);
+    f = (int)(warp - __ldg(p.facet_prefix + t));
+  }
+  const DevTask T = p.tasks[t];
+  const DevGrid G = p.grids[T.grid];
+  const DevReceiver R = p.receivers[T.receiver];
+  const int P = p.pool_size;
+
+  float3 origin, fnormal;
+  facet_geometry(T, f, origin, fnormal);
+  const Frame nframe = make_frame(fnormal, false);
+  const int g0 = __ldg(T.offsets + f);
+  const int g1 = __ldg(T.offsets + (f + 1) % P);
+  Frame sun;
+  sun.u = p.sun.u;
+  sun.n = p.sun.n;
+  sun.v = p.sun.v;
+  sun.identity = p.sun.identity != 0;
+
+  unsigned flags = 0;
+  double power = 0.0;
+  unsigned long long clamped = 0;
+  const int nl = p.light_end - p.light_begin;
+  for (int l = p.light_begin + lane; l < p.light_end; l += 32) {
+    const int a = (g0 + l) % P;
+    const float3 dir = to_world(sun, xyz(__ldg(p.samples + a)));
+    int32_t code;
+    if (collide(G, T.own, origin, dir, flags)) {
+      code = kShadowed;
+    } else {
+      const int b = (g1 + l) % P;
+      float3 n = normalize(to_world(nframe, xyz(__ldg(p.perturbations + b))));
+      float3 rd = normalize(reflect(neg(dir), n));
+      if (collide(G, T.own, origin, rd, flags)) {
+        code = kBlocked;
+      } else {
+        float tt, uu, vv;
+        if (!receiver_hit(R, origin, rd, tt, uu, vv)) {
+          code = kMissed;
+        } else {
+          float e = ray_energy(tt, rd, n, T.factor);
+          int row = int(uu * R.resolution.y);
+          int col = int(vv * R.resolution.x);
+          if (row >= R.resolution.y || col >= R.resolution.x || row < 0 || col < 0) {
+            row = min(max(row, 0), R.resolution.y - 1);
+            col = min(max(col, 0), R.resolution.x - 1);
+            ++clamped;
+          }
+          const int pix = row * R.resolution.x + col;
+          atomicAdd(R.image + pix, e);
+          power += (double)e;
+          code = pix;
+        }
+      }
+    }
+    if (kRecord) p.records[(size_t)(f - p.record_facet_begin) * nl + (l - p.light_begin)] = code;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    power += __shfl_down_sync(0xffffffffu, power, off);
+    clamped += __shfl_down_sync(0xffffffffu, clamped, off);
+  }
+  flags = __reduce_or_sync(0xffffffffu, flags);
+  if (lane == 0) {
+    if (power != 0.0) atomicAdd(p.power + T.power_slot, power);
+    if (clamped) atomicAdd(p.diag + kDiagClamped, clamped);
+    if (flags & 2u) atomicAdd(p.diag + kDiagDdaCap, 1ull);
+  }
+}
+
+__global__ void facets_kernel(DevTask T, float3* origins, float3* normals) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= T.num_facets) return;
+  float3 o, n;
+  facet_geometry(T, f, o, n);
+  origins[f] = o;
+  normals[f] = n;
+}
+
+}  // namespace
+
+cudaError_t QM_SYM(launch_facets)(const DevTask& task, float3* origins, float3* normals, cudaStream_t stream) {
+  if (task.num_facets <= 0) return cudaSuccess;
+  const int threads = 256;
+  facets_kernel<<<(task.num_facets + threads - 1) / threads, threads, 0, stream>>>(task, origins, normals);
+  return cudaGetLastError();
+}
+
+cudaError_t QM_SYM(launch_trace)(const TraceParams& p, bool record, cudaStream_t stream) {
+  const int threads = 256;
+  const long long warps = record ? (long long)(p.record_facet_end - p.record_facet_begin) : p.total_facets;
+  if (warps <= 0) return cudaSuccess;
+  const long long blocks = (warps + (threads / 32) - 1) / (threads / 32);
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+  if (record)
+    trace_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(p);
+  else
+    trace_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace qm

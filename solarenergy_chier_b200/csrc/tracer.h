@@ -1,0 +1,20 @@
+// Launchers of the sm_100a kernels, one symbol per compiled variant.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_scene.h"
+
+namespace qm {
+
+// tracer.cu built with FMA contraction (production) and without it
+// (every float operation rounded as the CPU oracle rounds it).
+cudaError_t launch_trace_fast(const TraceParams& p, bool record, cudaStream_t stream);
+cudaError_t launch_trace_exact(const TraceParams& p, bool record, cudaStream_t stream);
+
+// Micro-facet centres and normals of one heliostat, from the same device
+// function the tracer evaluates per facet.
+cudaError_t launch_facets_fast(const DevTask& task, float3* origins, float3* normals, cudaStream_t stream);
+cudaError_t launch_facets_exact(const DevTask& task, float3* origins, float3* normals, cudaStream_t stream);
+
+}  // namespace qm
