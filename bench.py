@@ -1,0 +1,323 @@
+"""Throughput benchmark of the plain tracer on the 624-heliostat field.
+
+Workload (the configuration the metric is quoted on): 624 focus-flat
+12.84 x 9.45 m heliostats (4x7 sub-heliostats, 0.02 m micro-facets, 300,664
+per heliostat, 187.6 M facets), radial-staggered 100-750 m north of a
+cylinder receiver (r 4 m, h 12 m, at 115 m; 1257x600 pixels), Buie sun shape
+CSR 0.1 from 128 x 2048 scrambled-Sobol samples, slope error 2.9 mrad, sun at
+azimuth 180 deg / elevation 60 deg, 20 m grid cells.  Synthetic, seeded
+(solarenergy_chier_b200.synth.large_field).
+
+One step = one launch tracing every facet of all 624 heliostats for
+`--passes` light indexes (default 32 of the 2048, 6.0e9 rays); successive
+steps take successive light ranges.  `value` is rays traced / device time
+(inputs resident in HBM); `e2e` is the same through the public API with the
+step's host inputs (both sample pools, pinned) copied in and the flux image
+and FP64 powers copied out inside the timed region.  The L2 cache (126 MB)
+is flushed before every step by writing a 256 MB buffer.
+
+Multi-GPU (torchrun): every rank traces the full field for its own light
+ranges (weak scaling, no collective inside the timed region); time is the
+maximum over ranks.
+
+--impl reference times the reference's own per-ray routine (its host code
+compiled from the reference tree, OpenMP over all host cores) on a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s at 624-heliostat field, batched vs plain at 1e-3 flux err; adjoint/fwd"
+UNIT = "Mrays/s"
+WORKLOAD = "624-heliostat focus-flat field, cylinder receiver 1257x600, plain tracer"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--passes", type=int, default=32, help="light indexes per step")
+    p.add_argument("--impl", default="native", choices=["native", "reference"])
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
+    p.add_argument("--exact", action="store_true", help="time the kernel build without FMA contraction")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def make_field(seed: int):
+    from solarenergy_chier_b200 import synth
+
+    out = Path(tempfile.mkdtemp(prefix="qmcrt_bench_"))
+    return synth.large_field(out, seed=seed)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self) -> dict:
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def fp32_peak_tflops(torch) -> float:
+    """Non-tensor FP32 FMA throughput of this GPU, measured (FMA = 2 flops)."""
+    from solarenergy_chier_b200 import microbench
+
+    return microbench.fp32_fma_tflops()
+
+
+def census(files, lights: int = 8, stride: int = 4001):
+    """Algorithmic work per ray on a fixed subsample, counted by the CPU oracle:
+    parallelogram tests reaching each stage, grid cells visited, receiver hits."""
+    from oracle import oracle as orc
+
+    import numpy as np
+
+    o = orc.OracleScene.from_files(files.scene, files.config)
+    P = o.pool_size
+    rng = np.random.default_rng(5)
+    th = 0.00465 * np.sqrt(rng.random(P))
+    ph = 2 * np.pi * rng.random(P)
+    dirs = np.stack([np.sin(th) * np.cos(ph), np.cos(th), np.sin(th) * np.sin(ph)], 1).astype(np.float32)
+    pert = np.tile(np.array([0, 1, 0], np.float32), (P, 1))
+    offs = {h: rng.integers(0, P, o.heliostat(h)["num_facets"] + 1).astype(np.int32) for h in range(o.num_heliostats)}
+    res = o.trace(list(range(o.num_heliostats)), dirs, pert, offs, 0, lights, facet_stride=stride, images=False)
+    c = res["counters"]
+    n = max(c["rays"], 1)
+    per = {k: c[k] / n for k in ("tests_det", "tests_u", "tests_v", "tests_t", "cells", "hit", "shadowed", "blocked",
+                                 "missed")}
+    # flops per ray credited per executed stage (23 det, 6 u, 15 v, 6 t), 20 per cell step,
+    # 70 for sampling/perturbation/reflection, 55 for the cylinder test when reached
+    reach_receiver = (c["hit"] + c["missed"]) / n
+    per["flops"] = (23 * per["tests_det"] + 6 * per["tests_u"] + 15 * per["tests_v"] + 6 * per["tests_t"]
+                    + 20 * per["cells"] + 70 + 55 * reach_receiver)
+    per["rays_sampled"] = n
+    return per
+
+
+def cpu_baseline(files, seconds: float):
+    """The reference's per-ray routine on all host cores (oracle/cpu_baseline.py),
+    in a child process."""
+    out = subprocess.run([sys.executable, "-m", "oracle.cpu_baseline", str(files.scene), str(files.config),
+                          str(seconds)], capture_output=True, text=True, cwd=str(ROOT), timeout=600)
+    if out.returncode != 0:
+        raise RuntimeError(out.stderr.strip().splitlines()[-1] if out.stderr.strip() else "cpu baseline failed")
+    return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    files = make_field(args.seed)
+    from oracle import refhost
+
+    if not refhost.available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference host library (oracle/_ref) was not built"}))
+        return
+    times, rays_total = [], 0
+    base = None
+    for step in range(args.warmup + args.steps):
+        b = cpu_baseline(files, max(2.0, 30.0 / max(args.steps, 1)))
+        if step >= args.warmup:
+            times.append(b)
+        base = b
+    value = statistics.mean(x["value"] for x in times)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded large_field)",
+            "config": {"workload": WORKLOAD + " (reference per-ray routine on host cores)",
+                       "global_batch": "sampled facets", "seq_len": None, "parallelism": "openmp"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": base["cores"], "kind": base["kind"],
+                             "sample": base["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+
+    import solarenergy_chier_b200 as q
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    files = make_field(args.seed)
+    scene = q.Scene(files.scene, files.config, device=local, seed=args.seed + 1000 * rank)
+    scene.set_math_mode(args.exact)
+    L = scene.lights_per_group
+    P = scene.pool_size
+    nh = scene.num_heliostats
+    ids = list(range(nh))
+    total_facets = scene.info.total_facets
+    passes = max(1, min(args.passes, L))
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def light_range(step):
+        k = (step * world + rank) % max(1, L // passes)
+        return k * passes, k * passes + passes
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident throughput -------------------------------------------
+    for step in range(args.warmup):
+        scene.set_light_range(*light_range(step))
+        scene.trace(ids, stream)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    t_wall = time.perf_counter()
+    for step in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(step))
+        scene.set_light_range(*light_range(args.warmup + step))
+        starts[step].record(stream)
+        scene.trace(ids, stream)
+        ends[step].record(stream)
+    barrier()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    kernel_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    rays_per_rank = total_facets * passes * args.steps
+    t = torch.tensor([kernel_ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    kernel_ms_max = float(t.item())
+    value = rays_per_rank * world / (kernel_ms_max / 1e3) / 1e6
+
+    # ---- end to end through the public API --------------------------------------
+    dirs, pert = scene.get_sample_pool()
+    h_dirs = torch.from_numpy(dirs).pin_memory()
+    h_pert = torch.from_numpy(pert).pin_memory()
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for step in range(e2e_steps):
+        scene.set_sample_pool(h_dirs.numpy(), h_pert.numpy())
+        scene.set_light_range(*light_range(step))
+        scene.trace(ids, stream)
+        img = scene.image(0)
+        per, total = scene.power()
+    e1.record(stream)
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    te = torch.tensor([e2e_ms], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = total_facets * passes * e2e_steps * world / (float(te.item()) / 1e3) / 1e6
+    h2d = 2 * P * 3 * 4 + nh * 4
+    d2h = img.nbytes + per.nbytes
+
+    if rank == 0:
+        per_ray = census(files)
+        fp32_peak = fp32_peak_tflops(torch)
+        achieved_tflops = value * 1e6 * per_ray["flops"] / 1e12
+        roofline = {"bound": "fp32", "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": achieved_tflops / fp32_peak if fp32_peak else None,
+                    "traffic": None,
+                    "peak_source": "measured in bench.py: non-tensor FP32 FMA microbenchmark on this GPU "
+                                   "(MEASURED_PEAKS.json holds no non-tensor FP32 figure)",
+                    "flops_per_ray": per_ray["flops"], "work_per_ray": per_ray,
+                    "kernel_ms_per_step": kernel_ms_max / args.steps}
+        prof = ROOT / "profiles" / "trace_kernel_traffic.json"
+        if prof.exists():
+            try:
+                roofline["traffic"] = json.loads(prof.read_text()).get("dram_bytes_per_launch")
+            except Exception:
+                pass
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": kernel_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "math_mode": "exact" if args.exact else "fast",
+                "data": "synthetic (seeded large_field: 624 heliostats, 187.6M micro-facets)",
+                "config": {"workload": WORKLOAD, "global_batch": f"{total_facets * passes * world} rays/step",
+                           "rays_per_step_per_gpu": total_facets * passes, "passes_per_step": passes,
+                           "seq_len": None, "parallelism": f"weak x{world} (light-index shards)",
+                           "l2": "flushed before every step (256 MB write)"},
+                "wall_s": wall, "clocks": clocks, "gpu_launches": args.steps,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": e2e_steps},
+                "roofline": roofline}
+        if not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline(files, args.cpu_seconds)
+            except Exception as exc:  # the reference library may be absent
+                line["cpu_baseline"] = {"value": None, "unavailable": str(exc)}
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -87,7 +87,10 @@ def build(force: bool = False) -> Path | None:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"reference build failed on {src}")
         objs.append(str(obj))
-    link = ["g++", "-shared", "-fopenmp", "-o", str(lib), *objs, "-Wl,--no-undefined"]
+    # -Bsymbolic: the reference code's CUDA runtime calls must bind to the host
+    # stand-ins linked into this library even when another library in the
+    # process (e.g. torch's libcudart) exports the same names globally.
+    link = ["g++", "-shared", "-fopenmp", "-o", str(lib), *objs, "-Wl,--no-undefined", "-Wl,-Bsymbolic"]
     r = subprocess.run(link, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -335,3 +335,71 @@ def mix32(x: int) -> int:
 
 def default_threads() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+
+
+# ---- single-routine probes (known-answer checks) ---------------------------
+def probe_heliostat(type_, size, gap, matrix, px, normal, pos, focus_length=-1.0, cap=1 << 16):
+    L = lib()
+    f3 = lambda v: np.ascontiguousarray(v, np.float32)  # noqa: E731
+    size, gap, normal, pos = f3(size), f3(gap), f3(normal), f3(pos)
+    matrix = np.ascontiguousarray(matrix, np.int32)
+    o = np.zeros((cap, 3), np.float32)
+    n = np.zeros((cap, 3), np.float32)
+    nsub = int(matrix[0] * matrix[1]) if type_ == 1 else 1
+    sv = np.zeros((3 * nsub, 3), np.float32)
+    lc = np.zeros((max(nsub, 1), 3), np.float32)
+    ln = np.zeros((max(nsub, 1), 3), np.float32)
+    counts = np.zeros(2, np.int32)
+    L.oracle_probe_heliostat.argtypes = [_i, _pf, _pf, _pi, _f, _pf, _pf, _f, _i, _pf, _pf, _pf, _pf, _pf, _pi]
+    rc = L.oracle_probe_heliostat(type_, _p(size, _f), _p(gap, _f), _p(matrix, _i), px, _p(normal, _f), _p(pos, _f),
+                                  focus_length, cap, _p(o, _f), _p(n, _f), _p(sv, _f), _p(lc, _f), _p(ln, _f),
+                                  _p(counts, _i))
+    if rc != 0:
+        raise ValueError("too many facets")
+    nf = int(counts[0])
+    return {"origins": o[:nf], "normals": n[:nf], "subverts": sv, "local_centers": lc, "local_normals": ln}
+
+
+def probe_cylinder_hit(pos, size, origin, direction):
+    L = lib()
+    L.oracle_probe_cylinder_hit.argtypes = [_pf, _pf, _pf, _pf, _pf]
+    a = [np.ascontiguousarray(v, np.float32) for v in (pos, size, origin, direction)]
+    tuv = np.zeros(3, np.float32)
+    hit = L.oracle_probe_cylinder_hit(*[_p(x, _f) for x in a], _p(tuv, _f))
+    return bool(hit), tuv
+
+
+def probe_cylinder_focus(pos, size, helio):
+    L = lib()
+    L.oracle_probe_cylinder_focus.argtypes = [_pf, _pf, _pf, _pf]
+    a = [np.ascontiguousarray(v, np.float32) for v in (pos, size, helio)]
+    out = np.zeros(3, np.float32)
+    L.oracle_probe_cylinder_focus(*[_p(x, _f) for x in a], _p(out, _f))
+    return out
+
+
+def probe_cylinder_resolution(size, ppm):
+    L = lib()
+    L.oracle_probe_cylinder_resolution.argtypes = [_pf, _i, _pi]
+    s = np.ascontiguousarray(size, np.float32)
+    out = np.zeros(2, np.int32)
+    L.oracle_probe_cylinder_resolution(_p(s, _f), ppm, _p(out, _i))
+    return tuple(int(x) for x in out)
+
+
+def probe_grid(pos, size, inter, helio_pos, helio_size, nsub, cap=1 << 16):
+    L = lib()
+    L.oracle_probe_grid.argtypes = [_pf, _pf, _pf, _i, _pf, _pf, _pi, _i, _pi, _pi, _pi]
+    p3 = [np.ascontiguousarray(v, np.float32) for v in (pos, size, inter)]
+    hp = np.ascontiguousarray(helio_pos, np.float32)
+    hs = np.ascontiguousarray(helio_size, np.float32)
+    ns = np.ascontiguousarray(nsub, np.int32)
+    index = np.zeros(cap, np.int32)
+    match = np.zeros(cap, np.int32)
+    counts = np.zeros(4, np.int32)
+    rc = L.oracle_probe_grid(*[_p(x, _f) for x in p3], len(ns), _p(hp, _f), _p(hs, _f), _p(ns, _i), cap,
+                             _p(index, _i), _p(match, _i), _p(counts, _i))
+    if rc != 0:
+        raise ValueError("grid too large")
+    ncell = int(counts[0] * counts[1] * counts[2])
+    return index[: ncell + 1], match[: counts[3]]

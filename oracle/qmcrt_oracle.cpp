@@ -991,3 +991,110 @@ void oracle_facet_offsets(uint32_t seed, uint32_t heliostat, int n, uint32_t poo
 uint32_t oracle_mix32(uint32_t x) { return oracle::mix(x); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Stand-alone probes of single reference routines, for the known-answer
+// checks of the reference's gtest suites (float arithmetic).
+extern "C" {
+
+// One heliostat with an explicit normal (no focus/sun step): lattice,
+// sub-heliostat table and micro-facets.  counts2 = (n_facets, n_sub).
+int oracle_probe_heliostat(int type, const float* size3, const float* gap2, const int* matrix2, float px,
+                           const float* normal3, const float* pos3, float focus_length, int cap, float* origins,
+                           float* normals, float* subverts, float* local_centers, float* local_normals,
+                           int* counts2) {
+  using namespace oracle;
+  Helio<float> h{};
+  h.type = type;
+  h.size = v3<float>(size3);
+  h.gap_x = gap2[0];
+  h.gap_y = gap2[1];
+  h.rows = matrix2[0];
+  h.cols = matrix2[1];
+  h.n_sub = type == 1 ? h.rows * h.cols : 1;
+  h.pixel_length = px;
+  h.normal = v3<float>(normal3);
+  h.pos = v3<float>(pos3);
+  h.focus_length = focus_length;
+  h.read_method = -1;
+  // Heliostat::CSetWorldVertex with the given normal (Heliostat.cu:25-40).
+  const V<float> s = h.size;
+  h.vertex[0] = mk<float>(-s.x / 2, s.y / 2, -s.z / 2);
+  h.vertex[1] = mk<float>(0, 0, s.z) + h.vertex[0];
+  h.vertex[2] = mk<float>(s.x, 0, s.z) + h.vertex[0];
+  h.vertex[3] = mk<float>(s.x, 0, 0) + h.vertex[0];
+  for (auto& v : h.vertex) v = rotate(v, h.normal, false) + h.pos;
+  helio_lattice(h);
+  std::vector<V<float>> sv;
+  helio_subverts(h, sv);
+  counts2[0] = h.n_facets;
+  counts2[1] = h.n_sub;
+  if (h.n_facets > cap) return -1;
+  for (int f = 0; f < h.n_facets; ++f) {
+    V<float> o, n;
+    facet(h, f, o, n);
+    origins[3 * f] = o.x, origins[3 * f + 1] = o.y, origins[3 * f + 2] = o.z;
+    normals[3 * f] = n.x, normals[3 * f + 1] = n.y, normals[3 * f + 2] = n.z;
+  }
+  for (size_t k = 0; k < sv.size(); ++k) subverts[3 * k] = sv[k].x, subverts[3 * k + 1] = sv[k].y, subverts[3 * k + 2] = sv[k].z;
+  for (size_t k = 0; k < h.lc.size(); ++k) {
+    local_centers[3 * k] = h.lc[k].x, local_centers[3 * k + 1] = h.lc[k].y, local_centers[3 * k + 2] = h.lc[k].z;
+    local_normals[3 * k] = h.ln[k].x, local_normals[3 * k + 1] = h.ln[k].y, local_normals[3 * k + 2] = h.ln[k].z;
+  }
+  return 0;
+}
+
+static oracle::Recv<float> probe_cylinder(const float* pos3, const float* size3) {
+  oracle::Recv<float> r{};
+  r.type = 1;
+  r.pos = oracle::v3<float>(pos3);
+  r.size = oracle::v3<float>(size3);
+  return r;
+}
+
+int oracle_probe_cylinder_hit(const float* pos3, const float* size3, const float* o, const float* d, float* tuv) {
+  auto r = probe_cylinder(pos3, size3);
+  float t = 0, u = 0, v = 0;
+  bool hit = oracle::cylinder_hit(r, oracle::v3<float>(o), oracle::v3<float>(d), t, u, v);
+  tuv[0] = t, tuv[1] = u, tuv[2] = v;
+  return hit ? 1 : 0;
+}
+
+void oracle_probe_cylinder_focus(const float* pos3, const float* size3, const float* helio3, float* out3) {
+  auto r = probe_cylinder(pos3, size3);
+  auto f = oracle::focus_of(r, oracle::v3<float>(helio3));
+  out3[0] = f.x, out3[1] = f.y, out3[2] = f.z;
+}
+
+void oracle_probe_cylinder_resolution(const float* size3, int ppm, int* out2) {
+  float pos[3] = {0, 0, 0};
+  auto r = probe_cylinder(pos, size3);
+  oracle::recv_init(r, ppm);
+  out2[0] = r.res_x, out2[1] = r.res_y;
+}
+
+// CGridHelioMatch for explicit heliostats (position, size, sub-heliostat count).
+int oracle_probe_grid(const float* pos3, const float* size3, const float* inter3, int n, const float* hpos,
+                      const float* hsize, const int* nsub, int cap, int* index, int* match, int* counts4) {
+  using namespace oracle;
+  Grid<float> g{};
+  g.pos = v3<float>(pos3);
+  g.size = v3<float>(size3);
+  g.inter = v3<float>(inter3);
+  g.start = 0;
+  g.count = n;
+  std::vector<Helio<float>> hs(n);
+  for (int i = 0; i < n; ++i) {
+    hs[i].pos = v3<float>(hpos + 3 * i);
+    hs[i].size = v3<float>(hsize + 3 * i);
+    hs[i].n_sub = nsub[i];
+  }
+  grid_match(g, hs);
+  counts4[0] = g.nx, counts4[1] = g.ny, counts4[2] = g.nz, counts4[3] = (int)g.match.size();
+  if ((int)g.index.size() > cap || (int)g.match.size() > cap) return -1;
+  std::copy(g.index.begin(), g.index.end(), index);
+  std::copy(g.match.begin(), g.match.end(), match);
+  return 0;
+}
+
+}  // extern "C"

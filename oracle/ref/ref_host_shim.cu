@@ -26,6 +26,7 @@
 #include <cstring>
 #include <exception>
 #include <iostream>
+#include <memory>
 #include <random>
 #include <sstream>
 #include <stdexcept>
@@ -384,22 +385,32 @@ void ref_trace(const RefTraceArgs* a) {
   const long long total_pix = a->images ? a->image_base[s->getReceivers().size()] : 0;
   long long totals[6] = {0};
   if (a->threads > 0) omp_set_num_threads(a->threads);
+  // Sub-heliostat vertex table of each grid (setFlatRectangleHeliostatVertexs), built once.
+  std::vector<std::vector<float3>> grid_verts(s->getGrids().size());
+  for (size_t gi = 0; gi < s->getGrids().size(); ++gi) {
+    Grid* g = s->getGrids()[gi];
+    for (int k = g->getStartHeliostatIndex(); k < g->getStartHeliostatIndex() + g->getNumberOfHeliostats(); ++k)
+      s->getHeliostats()[k]->CGetSubHeliostatVertexes(grid_verts[gi]);
+  }
   for (int ti = 0; ti < a->n_ids; ++ti) {
     const int hid = a->ids[ti];
     Heliostat* h = s->getHeliostats()[hid];
     auto* g = static_cast<RectangleGrid*>(s->getGrids()[h->getBelongingGridId()]);
     const int rid = g->getBelongingReceiverIndex();
     Receiver* rc = s->getReceivers()[rid];
-    std::vector<float3> verts;
-    for (int k = g->getStartHeliostatIndex(); k < g->getStartHeliostatIndex() + g->getNumberOfHeliostats(); ++k)
-      s->getHeliostats()[k]->CGetSubHeliostatVertexes(verts);
+    const std::vector<float3>& verts = grid_verts[h->getBelongingGridId()];
     const HeliostatArgument arg(nullptr, nullptr, nullptr, 0, sub_begin_of(hid), h->getSubHelioSize());
     // QuasiMonteCarloRayTracer::rayTracing (QuasiMonteCarloRayTracer.cpp:58-60).
     float ratio = h->getPixelLength() / rc->getPixelLength();
     float factor = cfg->getDni() * ratio * ratio * cfg->getReflected_rate() / float(L);
-    std::vector<float3> O, N;
-    all_facets(h, O, N);
-    const int n = (int)O.size();
+    int2 src;
+    float2 len;
+    int n;
+    lattice(h, src, len, n);
+    // Facet centres/normals are evaluated only for the facets traced; the
+    // flat-heliostat host function writes element f of full-size arrays.
+    std::unique_ptr<float3[]> O(new float3[std::max(n, 1)]), N(new float3[std::max(n, 1)]);
+    const bool flat = Heliostat_type(h) == 0;
     const int* off = a->offsets + a->offset_base[hid];
     const int2 res = rc->getResolution();
 #pragma omp parallel
@@ -410,6 +421,12 @@ void ref_trace(const RefTraceArgs* a) {
 #pragma omp for schedule(dynamic, 64)
       for (int f = 0; f < n; ++f) {
         if (a->facet_stride > 1 && f % a->facet_stride != a->facet_phase) continue;
+        if (flat)
+          host_map_microhelio_center_and_normal(f, O.get(), N.get(), h->getNormal(), h->getSize(),
+                                                h->getRowAndColumn(), src, h->getPixelLength(), h->getGap(),
+                                                h->getPosition(), (size_t)n);
+        else
+          facet(h, f, src, len, n, O[f], N[f]);
         const float3 origin = O[f];
         for (int l = a->light_begin; l < a->light_end; ++l) {
           ++cnt[0];
@@ -473,6 +490,7 @@ void ref_trace(const RefTraceArgs* a) {
 // trimmed_mean's loop (Tool/Smoother/ImageSmoother.cu:13-64) on the
 // reference's own Max_heap / Min_heap (heap.cuh).
 void ref_smooth(const float* in, float* out, int width, int height, int kernel_radius, float trimmed_ratio) {
+  Quiet quiet;
   std::streambuf* old = std::cout.rdbuf(nullptr);
 #pragma omp parallel for schedule(static)
   for (int y = 0; y < height; ++y) {

@@ -40,6 +40,7 @@ CUDA_UNITS = [
     ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-fmad=false"]),
     ("pools.cu", "pools.o", []),
     ("smooth.cu", "smooth.o", []),
+    ("microbench.cu", "microbench.o", []),
 ]
 
 
@@ -62,7 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     """Compile every unit whose inputs changed and link libqmcrt.so and bin/qmcrt."""
     OBJ.mkdir(exist_ok=True)
     EXE.parent.mkdir(exist_ok=True)
-    headers = sorted(CSRC.glob("*.h")) + [INCLUDE / "qmcrt.h"]
+    headers = sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
     objects = []
     for src in HOST_SOURCES:
         obj = OBJ / (Path(src).stem + ".o")
@@ -75,13 +76,15 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         cmd = [NVCC, *NVCC_FLAGS, *flags, f"-I{CSRC}", f"-I{INCLUDE}", "-c", str(CSRC / src), "-o", str(obj)]
         _compile(obj, [CSRC / src, *headers], cmd, force, verbose)
         objects.append(obj)
-    link = [NVCC, *ARCH, "-shared", "-o", str(LIB), *map(str, objects), "-lcudart"]
+    # The CUDA runtime is linked statically: the library does not depend on
+    # whichever libcudart.so.12 another package (e.g. torch) loaded first.
+    link = [NVCC, *ARCH, "-shared", "--cudart", "static", "-o", str(LIB), *map(str, objects)]
     _link(LIB, objects, link, force, verbose)
     main_obj = OBJ / "main.o"
     _compile(main_obj, [CSRC / "main.cpp", INCLUDE / "qmcrt.h"],
              ["g++", *HOST_FLAGS, f"-I{INCLUDE}", "-c", str(CSRC / "main.cpp"), "-o", str(main_obj)], force, verbose)
     _link(EXE, [main_obj, LIB], ["g++", "-o", str(EXE), str(main_obj), f"-L{PKG}", "-lqmcrt",
-                                  f"-Wl,-rpath,$ORIGIN/..", f"-L{CUDA_HOME / 'lib64'}", "-lcudart"], force, verbose)
+                                  "-Wl,-rpath,$ORIGIN/.."], force, verbose)
     return LIB
 
 

@@ -1,0 +1,93 @@
+// Roofline denominators measured on the running GPU: non-tensor FP32 FMA
+// throughput and L2 float-atomic throughput (include/qmcrt_bench.h).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "qmcrt_bench.h"
+
+namespace {
+
+__global__ void fma_kernel(float* out, int iters, float a, float b) {
+  float x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+    x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+    x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+  }
+  float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+__global__ void atomic_kernel(float* img, int n_pix, int per_thread, uint32_t salt) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int i = 0; i < per_thread; ++i) {
+    uint32_t h = (t * 0x9e3779b1u) ^ (i * 0x85ebca6bu) ^ salt;
+    h ^= h >> 15;
+    h *= 0x2c1b3c6du;
+    h ^= h >> 12;
+    atomicAdd(img + (h % (uint32_t)n_pix), 1.0f);
+  }
+}
+
+float time_launch(void (*launch)(void*), void* ctx) {
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  launch(ctx);  // warm-up
+  cudaEventRecord(a);
+  launch(ctx);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return ms;
+}
+
+struct FmaCtx {
+  float* out;
+  int blocks, threads, iters;
+};
+void fma_launch(void* p) {
+  auto* c = static_cast<FmaCtx*>(p);
+  fma_kernel<<<c->blocks, c->threads>>>(c->out, c->iters, 0.999f, 0.001f);
+}
+
+struct AtomCtx {
+  float* img;
+  int n_pix, blocks, threads, per_thread;
+};
+void atom_launch(void* p) {
+  auto* c = static_cast<AtomCtx*>(p);
+  atomic_kernel<<<c->blocks, c->threads>>>(c->img, c->n_pix, c->per_thread, 17u);
+}
+
+}  // namespace
+
+extern "C" int qmcrt_microbench_fp32(double* tflops) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  FmaCtx c{nullptr, sms * 16, 256, 1 << 14};
+  if (cudaMalloc(&c.out, sizeof(float) * c.blocks * c.threads) != cudaSuccess) return 3;
+  float ms = time_launch(fma_launch, &c);
+  cudaFree(c.out);
+  if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return 3;
+  double flops = 2.0 * 8.0 * (double)c.iters * c.blocks * c.threads;
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  return 0;
+}
+
+extern "C" int qmcrt_microbench_atomics(int n_pixels, double* giga_per_s) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  AtomCtx c{nullptr, n_pixels, sms * 8, 256, 256};
+  if (n_pixels <= 0 || cudaMalloc(&c.img, sizeof(float) * n_pixels) != cudaSuccess) return 3;
+  cudaMemset(c.img, 0, sizeof(float) * n_pixels);
+  float ms = time_launch(atom_launch, &c);
+  cudaFree(c.img);
+  if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return 3;
+  *giga_per_s = (double)c.blocks * c.threads * c.per_thread / (ms * 1e-3) / 1e9;
+  return 0;
+}

@@ -17,9 +17,12 @@
 // parallelograms tested.  The box is conservative (padding far above float
 // rounding) so the any-hit answer is unchanged.
 //
-// This file is compiled twice: QM_TRACE_VARIANT=exact with -fmad=false (each
-// float operation rounds as in the CPU oracle) and QM_TRACE_VARIANT=fast with
-// FMA contraction (production).
+// Everything outside the grid walk (sampling, facet geometry, slope error,
+// reflection, receiver intersection, energy) uses explicitly rounded
+// operations (qs::), so it rounds exactly as the CPU oracle does in both
+// builds.  The grid walk and its blocker tests (qm::) are compiled twice:
+// QM_TRACE_VARIANT=exact with -fmad=false, and QM_TRACE_VARIANT=fast with FMA
+// contraction (production).
 #include <climits>
 
 #include "device_scene.h"
@@ -135,38 +138,42 @@ __device__ bool collide(const DevGrid& g, int own, float3 o, float3 d, unsigned&
   return false;
 }
 
-// CylinderReceiver::GIntersect (Scene/DataStructure/Receiver/CylinderReceiver.cuh:39-89).
+// CylinderReceiver::GIntersect (Scene/DataStructure/Receiver/CylinderReceiver.cuh:39-89),
+// every operation explicitly rounded: delta = |Ro|^2 - tp^2 cancels
+// catastrophically for far heliostats (|Ro|^2 ~ 5e5 m^2, float spacing
+// 0.03 m^2), so a fused multiply-add there would move rays across the
+// cylinder's silhouette relative to the reference's rounding.
 // acos takes its argument clamped to [-1, 1]; the reference prints an error
 // and lets a NaN through when rounding pushes it outside.
 __device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
-  float2 l = make_float2(o.x - r.pos.x, o.z - r.pos.z);
-  if (dot2(l, l) <= r.size.x * r.size.x) return false;
-  float2 ro = make_float2(r.pos.x - o.x, r.pos.z - o.z);
-  float tp = dot2(ro, normalize2(make_float2(d.x, d.z)));
-  float delta = dot2(ro, ro) - tp * tp;
-  float r2 = r.size.x * r.size.x;
+  float2 l = make_float2(qm_rn_sub(o.x, r.pos.x), qm_rn_sub(o.z, r.pos.z));
+  const float r2 = qm_rn_mul(r.size.x, r.size.x);
+  if (qs::dot2(l, l) <= r2) return false;
+  float2 ro = make_float2(qm_rn_sub(r.pos.x, o.x), qm_rn_sub(r.pos.z, o.z));
+  float tp = qs::dot2(ro, qs::normalize2(make_float2(d.x, d.z)));
+  float delta = qm_rn_sub(qs::dot2(ro, ro), qm_rn_mul(tp, tp));
   if ((double)tp < -kEps || delta > r2) return false;
-  float t_plus = delta <= 0.0f ? r.size.x : sqrtf(r2 - delta);
-  t = (tp - t_plus) / length2(make_float2(d.x, d.z));
-  float3 ip = add(mul(d, t), o);
-  u = (ip.y - r.pos.y) / r.size.y + 0.5f;
+  float t_plus = delta <= 0.0f ? r.size.x : sqrtf(qm_rn_sub(r2, delta));
+  t = qm_rn_div(qm_rn_sub(tp, t_plus), qs::length2(make_float2(d.x, d.z)));
+  float3 ip = qs::add(qs::mul(d, t), o);
+  u = qm_rn_add(qm_rn_div(qm_rn_sub(ip.y, r.pos.y), r.size.y), 0.5f);
   if (u < 0.0f || u > 1.0f) return false;
-  float2 cs = normalize2(make_float2(ip.x - r.pos.x, ip.z - r.pos.z));
+  float2 cs = qs::normalize2(make_float2(qm_rn_sub(ip.x, r.pos.x), qm_rn_sub(ip.z, r.pos.z)));
   float cx = fminf(fmaxf(cs.x, -1.0f), 1.0f);
-  v = (float)((double)acosf(cx) / (2 * M_PI));
-  if (cs.y < 0) v = 1 - v;
+  v = (float)__ddiv_rn((double)acosf(cx), 2 * M_PI);
+  if (cs.y < 0) v = qm_rn_sub(1.0f, v);
   return true;
 }
 
 __device__ __forceinline__ bool receiver_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
-  if (r.type == 0) return ray_parallelogram(o, d, r.a, r.ab, r.ac, t, u, v);
+  if (r.type == 0) return qs::ray_parallelogram(o, d, r.a, r.ab, r.ac, t, u, v);
   return cylinder_hit(r, o, d, t, u, v);
 }
 
 // Micro-facet centre and normal (rectangle_heliostat::map_microhelio_center_and_normal,
 // Scene/DataStructure/Heliostat/RectangleHelio.cu:54-80; focusFlatRectangle_heliostat
 // kernels, FocusFlatRectangleHelio.cu:12-64), evaluated per facet instead of
-// materialised.
+// materialised; explicitly rounded (once per facet, off the hot path).
 __device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& origin, float3& normal) {
   Frame hf;
   hf.u = T.fu;
@@ -176,14 +183,17 @@ __device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& 
   const int per_row = T.row_col.y * T.sub_row_col.y;
   int row = f / per_row;
   int col = f % per_row;
+  const float px = T.pixel_length;
   if (T.type == 0) {
     int brow = row / T.sub_row_col.x;
     int bcol = col / T.sub_row_col.y;
     float3 c;
-    c.x = col * T.pixel_length + bcol * T.gap.x + T.pixel_length / 2 - T.size.x / 2;
+    c.x = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)col, px), qm_rn_mul((float)bcol, T.gap.x)), px / 2),
+                    T.size.x / 2);
     c.y = T.size.y / 2;
-    c.z = row * T.pixel_length + brow * T.gap.y + T.pixel_length / 2 - T.size.z / 2;
-    origin = add(to_world(hf, c), T.pos);
+    c.z = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)row, px), qm_rn_mul((float)brow, T.gap.y)), px / 2),
+                    T.size.z / 2);
+    origin = qs::add(qs::to_world(hf, c), T.pos);
     normal = T.normal;
   } else {
     int block = (row / T.sub_row_col.x) * T.row_col.y + col / T.sub_row_col.y;
@@ -191,11 +201,11 @@ __device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& 
     float3 lc = T.local_centers[block];
     row %= T.sub_row_col.x;
     col %= T.sub_row_col.y;
-    float3 lp = make_float3((col + 0.5f) * T.pixel_length - T.sub_length.y / 2, 0.0f,
-                            (row + 0.5f) * T.pixel_length - T.sub_length.x / 2);
-    lp = add(rotate_to(lp, ln, true), lc);
-    normal = to_world(hf, ln);
-    origin = add(to_world(hf, lp), T.pos);
+    float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)col, 0.5f), px), T.sub_length.y / 2), 0.0f,
+                            qm_rn_sub(qm_rn_mul(qm_rn_add((float)row, 0.5f), px), T.sub_length.x / 2));
+    lp = qs::add(qs::rotate_to(lp, ln, true), lc);
+    normal = qs::to_world(hf, ln);
+    origin = qs::add(qs::to_world(hf, lp), T.pos);
   }
 }
 
@@ -229,7 +239,7 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams p) {
 
   float3 origin, fnormal;
   facet_geometry(T, f, origin, fnormal);
-  const Frame nframe = make_frame(fnormal, false);
+  const Frame nframe = qs::make_frame(fnormal, false);
   const int g0 = __ldg(T.offsets + f);
   const int g1 = __ldg(T.offsets + (f + 1) % P);
   Frame sun;
@@ -244,14 +254,14 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams p) {
   const int nl = p.light_end - p.light_begin;
   for (int l = p.light_begin + lane; l < p.light_end; l += 32) {
     const int a = (g0 + l) % P;
-    const float3 dir = to_world(sun, xyz(__ldg(p.samples + a)));
+    const float3 dir = qs::to_world(sun, xyz(__ldg(p.samples + a)));
     int32_t code;
     if (collide(G, T.own, origin, dir, flags)) {
       code = kShadowed;
     } else {
       const int b = (g1 + l) % P;
-      float3 n = normalize(to_world(nframe, xyz(__ldg(p.perturbations + b))));
-      float3 rd = normalize(reflect(neg(dir), n));
+      float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(p.perturbations + b))));
+      float3 rd = qs::normalize(qs::reflect(neg(dir), n));
       if (collide(G, T.own, origin, rd, flags)) {
         code = kBlocked;
       } else {
@@ -259,9 +269,9 @@ __global__ void __launch_bounds__(256) trace_kernel(TraceParams p) {
         if (!receiver_hit(R, origin, rd, tt, uu, vv)) {
           code = kMissed;
         } else {
-          float e = ray_energy(tt, rd, n, T.factor);
-          int row = int(uu * R.resolution.y);
-          int col = int(vv * R.resolution.x);
+          float e = qs::ray_energy(tt, rd, n, T.factor);
+          int row = int(qm_rn_mul(uu, (float)R.resolution.y));
+          int col = int(qm_rn_mul(vv, (float)R.resolution.x));
           if (row >= R.resolution.y || col >= R.resolution.x || row < 0 || col < 0) {
             row = min(max(row, 0), R.resolution.y - 1);
             col = min(max(col, 0), R.resolution.x - 1);

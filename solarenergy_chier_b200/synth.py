@@ -1,0 +1,145 @@
+"""Seeded synthetic scenes in the reference's file formats (.scn, .json, task file).
+
+There is no public data set for this path; these generators stand in for
+the benchmark fields.  Conventions: x = east, y = up, z = north; the tower
+stands at the origin and the field lies north of it.  The sun direction is
+the direction of travel, -(cos e sin a, sin e, cos e cos a) for azimuth a
+(clockwise from north) and elevation e.
+
+  small_field   50 flat 4x4 m heliostats on a jittered 10x5 lattice (8 m
+                pitch), 8x6 m rectangle receiver at 80 m (vertical, facing
+                the field: the scene format has no receiver tilt), 0.05 m
+                micro-facets (6400 per heliostat), 10 m grid cells,
+                0.05 m receiver pixels (160x120).
+  large_field   624 focus-flat 12.84x9.45 m heliostats (4x7 sub-heliostats,
+                no gap, focal length = slant range) on radial-staggered rings
+                100-750 m over +-70 degrees, cylinder receiver r = 4 m,
+                h = 12 m at 115 m, 0.02 m micro-facets (300,664 per
+                heliostat), 20 m grid cells, 0.02 m receiver pixels (1257x600).
+"""
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+
+def sun_direction(azimuth_deg: float, elevation_deg: float) -> list[float]:
+    a, e = math.radians(azimuth_deg), math.radians(elevation_deg)
+    return [-(math.cos(e) * math.sin(a)), -math.sin(e), -(math.cos(e) * math.cos(a))]
+
+
+@dataclass
+class SceneFiles:
+    scene: Path
+    config: Path
+    tasks: Path
+    num_heliostats: int
+
+
+def _fmt(x: float) -> str:
+    return f"{x:.6f}"
+
+
+def _write(out_dir: Path, name: str, recv_lines: list[str], grid: dict, helio_block: list[str],
+           positions: np.ndarray, size: tuple, config: dict) -> SceneFiles:
+    out_dir = Path(out_dir)
+    out_dir.mkdir(parents=True, exist_ok=True)
+    lines = ["# synthetic scene " + name, "ground\t4096.000000\t4096.000000", "ngrid\t1", ""]
+    lines += recv_lines + [""]
+    lines += ["Grid\t0",
+              "pos\t\t" + "\t".join(_fmt(v) for v in grid["pos"]),
+              "size\t" + "\t".join(_fmt(v) for v in grid["size"]),
+              "inter\t" + "\t".join(_fmt(v) for v in grid["inter"]),
+              f"n\t\t{len(positions)}", f"type\t{grid['helio_type']}", "end", ""]
+    lines += helio_block
+    for p in positions:
+        lines.append("helio\t" + "\t".join(_fmt(v) for v in p))
+        lines.append("\t\t" + "\t".join(_fmt(v) for v in size))
+    scene = out_dir / f"{name}_scene.scn"
+    scene.write_text("\n".join(lines) + "\n")
+    cfg = out_dir / f"{name}_configuration.json"
+    cfg.write_text(json.dumps(config, indent=2) + "\n")
+    tasks = out_dir / f"{name}_heliostat_index.txt"
+    tasks.write_text(f"{len(positions)}\n" + " ".join(str(i) for i in range(len(positions))) + "\n")
+    return SceneFiles(scene, cfg, tasks, len(positions))
+
+
+def small_field(out_dir, seed: int = 0, helio_pixel: float = 0.05, receiver_pixel: float = 0.05,
+                groups: int = 128, per_group: int = 2048, rows: int = 5, cols: int = 10) -> SceneFiles:
+    """The 50-heliostat flat field (optionally coarser facets / smaller lattice for tests)."""
+    rng = np.random.default_rng(seed)
+    pitch = 8.0
+    xs = (np.arange(cols) - (cols - 1) / 2.0) * pitch
+    zs = 40.0 + np.arange(rows) * pitch
+    pos = []
+    for z in zs:
+        for x in xs:
+            jx, jz = rng.uniform(-0.5, 0.5, 2)
+            pos.append([x + jx, 2.5, z + jz])
+    pos = np.array(pos)
+    recv = ["Recv\t0", "pos\t\t0.000000\t80.000000\t0.000000", "size\t8.000000\t6.000000\t0.100000",
+            "norm\t0.000000\t0.000000\t1.000000", "face\t0", "end"]
+    x0 = float(np.floor(pos[:, 0].min() - 10.0))
+    z0 = float(np.floor(pos[:, 2].min() - 10.0))
+    grid = {"pos": [x0, 0.0, z0], "size": [float(np.ceil(pos[:, 0].max() + 10.0 - x0)), 10.0,
+                                            float(np.ceil(pos[:, 2].max() + 10.0 - z0))],
+            "inter": [10.0, 10.0, 10.0], "helio_type": 0}
+    config = {"sun_dir": sun_direction(180.0, 60.0), "dni": 1000.0, "csr": 0.1, "num_of_sunshape_groups": groups,
+              "num_per_sunshape_group": per_group, "inverse_transform_sampling_groups": 1024,
+              "receiver_pixel_length": receiver_pixel, "helio_disturb_std": 0.002,
+              "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
+    return _write(out_dir, "small", recv, grid, ["gap\t0.000000\t0.000000", "matrix\t1\t1"], pos,
+                  (4.0, 0.1, 4.0), config)
+
+
+def radial_staggered(n: int, r_min: float, r_max: float, span_deg: float, seed: int) -> np.ndarray:
+    """n (x, z) positions on staggered rings between r_min and r_max over +-span_deg
+    around north, with seeded jitter."""
+    rng = np.random.default_rng(seed)
+    ring_step = 30.0
+    radii = np.arange(r_min, r_max + 1e-6, ring_step)
+    span = math.radians(2 * span_deg)
+    arc_total = span * radii.sum()
+    spacing = arc_total / n
+    pos = []
+    for k, r in enumerate(radii):
+        m = max(1, int(round(span * r / spacing)))
+        offset = 0.5 if k % 2 else 0.0
+        for j in range(m):
+            az = -math.radians(span_deg) + span * (j + 0.25 + 0.5 * offset) / m
+            pos.append((r, az))
+    pos = np.array(pos)
+    if len(pos) > n:
+        keep = np.sort(rng.choice(len(pos), n, replace=False))
+        pos = pos[keep]
+    while len(pos) < n:  # top up on the outermost ring
+        az = rng.uniform(-math.radians(span_deg), math.radians(span_deg))
+        pos = np.vstack([pos, [r_max, az]])
+    r = pos[:, 0] + rng.uniform(-1.0, 1.0, n)
+    az = pos[:, 1] + rng.uniform(-1.0, 1.0, n) / pos[:, 0]
+    return np.stack([r * np.sin(az), r * np.cos(az)], axis=1)
+
+
+def large_field(out_dir, seed: int = 0, num_heliostats: int = 624, helio_pixel: float = 0.02,
+                receiver_pixel: float = 0.02, groups: int = 128, per_group: int = 2048,
+                rows: int = 4, cols: int = 7) -> SceneFiles:
+    """The 624-heliostat focus-flat field with a cylinder receiver."""
+    xz = radial_staggered(num_heliostats, 100.0, 750.0, 70.0, seed)
+    pos = np.stack([xz[:, 0], np.full(len(xz), 5.5), xz[:, 1]], axis=1)
+    recv = ["Recv\t1", "pos\t\t0.000000\t115.000000\t0.000000", "size\t4.000000\t12.000000\t0.000000",
+            "norm\t0.000000\t1.000000\t0.000000", "face\t0", "end"]
+    x0 = float(np.floor(pos[:, 0].min() - 20.0))
+    z0 = float(np.floor(pos[:, 2].min() - 20.0))
+    grid = {"pos": [x0, 0.0, z0], "size": [float(np.ceil(pos[:, 0].max() + 20.0 - x0)), 20.0,
+                                            float(np.ceil(pos[:, 2].max() + 20.0 - z0))],
+            "inter": [20.0, 20.0, 20.0], "helio_type": 1}
+    config = {"sun_dir": sun_direction(180.0, 60.0), "dni": 1000.0, "csr": 0.1, "num_of_sunshape_groups": groups,
+              "num_per_sunshape_group": per_group, "inverse_transform_sampling_groups": 1024,
+              "receiver_pixel_length": receiver_pixel, "helio_disturb_std": 0.0029,
+              "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
+    block = ["gap\t0.000000\t0.000000", f"matrix\t{rows}\t{cols}", "surface_property -1 -1 -1 -1 -1 -1"]
+    return _write(out_dir, "large", recv, grid, block, pos, (12.84, 0.1, 9.45), config)
