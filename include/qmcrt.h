@@ -153,6 +153,17 @@ int qmcrt_debug_hit_records(qmcrt_scene* scene, int heliostat, int facet_begin, 
  * in-place trimmed mean of a device image.  0 <= trim_ratio < 0.5. */
 int qmcrt_smooth(float* device_image, int width, int height, int radius, float trim_ratio, void* stream);
 
+/* No counterpart in the reference.  qmcrt_smooth without any device
+ * allocation, for callers that may not call cudaMalloc (a fixed device-memory
+ * budget already reserved by another allocator, or a real-time loop that
+ * cannot take an allocation's latency or failure).  The image copy lives in a
+ * static device array of 4,194,304 floats (16 MiB) that every GPU loading the
+ * library holds until exit; larger images fail with QMCRT_ERR_INVALID.  The
+ * first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race. */
+int qmcrt_smooth_static(float* device_image, int width, int height, int radius, float trim_ratio, void* stream);
+
 /* Replaces TaskLoader::loadRayTracingHeliostatIndex (RayTracingPipeline/TaskLoader.cpp:114-204).
  * status: 1 true, 0 false (repeated or surplus indexes).  receivers receives the
  * grid ids of the listed heliostats, as the reference records them. */

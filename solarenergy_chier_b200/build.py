@@ -41,6 +41,7 @@ CUDA_UNITS = [
     ("pools.cu", "pools.o", []),
     ("smooth.cu", "smooth.o", []),
     ("microbench.cu", "microbench.o", []),
+    ("smooth_static.cu", "smooth_static.o", []),
 ]
 
 

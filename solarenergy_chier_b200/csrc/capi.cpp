@@ -107,6 +107,10 @@ class DeviceGuard {
 
 }  // namespace
 
+namespace qm {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace qm
+
 struct qmcrt_scene {
   int device = 0;
   unsigned seed = 0;
