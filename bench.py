@@ -57,6 +57,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--exact", action="store_true", help="time the kernel build without FMA contraction")
+    p.add_argument("--mode", type=int, default=None, help="kernel build: 0 production, 1 exact, 2 production/48 regs")
+    p.add_argument("--heliostats", type=int, default=0, help="trace only the first N heliostats (profiling)")
     return p.parse_args()
 
 
@@ -205,12 +207,13 @@ def main():
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     files = make_field(args.seed)
     scene = q.Scene(files.scene, files.config, device=local, seed=args.seed + 1000 * rank)
-    scene.set_math_mode(args.exact)
+    mode = args.mode if args.mode is not None else (1 if args.exact else 0)
+    scene.set_math_mode(mode)
     L = scene.lights_per_group
     P = scene.pool_size
     nh = scene.num_heliostats
-    ids = list(range(nh))
-    total_facets = scene.info.total_facets
+    ids = list(range(nh if args.heliostats <= 0 else min(nh, args.heliostats)))
+    total_facets = sum(scene.heliostat(h)["num_facets"] for h in ids)
     passes = max(1, min(args.passes, L))
     stream = torch.cuda.Stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -298,7 +301,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": kernel_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "math_mode": "exact" if args.exact else "fast",
+                "math_mode": {0: "fast", 1: "exact", 2: "fast-48reg"}[mode],
                 "data": "synthetic (seeded large_field: 624 heliostats, 187.6M micro-facets)",
                 "config": {"workload": WORKLOAD, "global_batch": f"{total_facets * passes * world} rays/step",
                            "rays_per_step_per_gpu": total_facets * passes, "passes_per_step": passes,

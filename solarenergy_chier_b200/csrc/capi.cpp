@@ -131,6 +131,7 @@ struct qmcrt_scene {
   std::vector<qm::DevTask> templates;
   DBuf d_tasks, d_prefix;
   std::vector<int> cached_ids;
+  long long cached_lights = -1;
   bool cache_valid = false;
   qm::DevTask* h_stage = nullptr;  // pinned staging for task uploads
   long long* h_prefix = nullptr;
@@ -474,22 +475,34 @@ qm::TraceParams base_params(qmcrt_scene* s) {
 }
 
 cudaError_t run_trace(qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st) {
-  return s->exact ? qm::launch_trace_exact(p, record, st) : qm::launch_trace_fast(p, record, st);
+  switch (s->exact) {
+    case 1: return qm::launch_trace_exact(p, record, st);
+    case 2: return qm::launch_trace_fast4(p, record, st);
+    default: return qm::launch_trace_fast(p, record, st);
+  }
 }
 
 void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
   if (n < 0 || (n > 0 && !ids)) invalid("heliostat list is invalid");
   for (int i = 0; i < n; ++i) check_heliostat(s, ids[i]);
   if (n == 0) return;
+  for (int i = 0; i < n; ++i)
+    if ((long long)s->templates[ids[i]].num_facets * (s->light_end - s->light_begin) >= 0x7fffffffLL)
+      invalid("a heliostat's micro-facets x lights must stay below 2^31 rays per launch; trace fewer lights");
   DeviceGuard guard(s->device);
-  bool same = s->cache_valid && (int)s->cached_ids.size() == n && std::equal(ids, ids + n, s->cached_ids.begin());
+  const long long nl = s->light_end - s->light_begin;
+  if (nl == 0) return;
+  const long long chunk = qm::trace_chunk_rays_fast();
+  auto chunks_of = [&](int id) { return ((long long)s->templates[id].num_facets * nl + chunk - 1) / chunk; };
+  bool same = s->cache_valid && s->cached_lights == nl && (int)s->cached_ids.size() == n &&
+              std::equal(ids, ids + n, s->cached_ids.begin());
   long long total = 0;
   if (!same) {
     ensure_stage(s, (size_t)n);
     s->h_prefix[0] = 0;
     for (int i = 0; i < n; ++i) {
       s->h_stage[i] = s->templates[ids[i]];
-      s->h_prefix[i + 1] = s->h_prefix[i] + s->templates[ids[i]].num_facets;
+      s->h_prefix[i + 1] = s->h_prefix[i] + chunks_of(ids[i]);
     }
     cuda_check(cudaMemcpyAsync(s->d_tasks.p, s->h_stage, n * sizeof(DevTask), cudaMemcpyHostToDevice, stream),
                "task upload");
@@ -498,9 +511,10 @@ void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
     if (!s->stage_done) cuda_check(cudaEventCreateWithFlags(&s->stage_done, cudaEventDisableTiming), "cudaEventCreate");
     cuda_check(cudaEventRecord(s->stage_done, stream), "cudaEventRecord");
     s->cached_ids.assign(ids, ids + n);
+    s->cached_lights = nl;
     s->cache_valid = true;
   }
-  for (int i = 0; i < n; ++i) total += s->templates[ids[i]].num_facets;
+  for (int i = 0; i < n; ++i) total += chunks_of(ids[i]);
   qm::TraceParams p = base_params(s);
   p.tasks = s->d_tasks.as<DevTask>();
   p.facet_prefix = s->d_prefix.as<long long>();
@@ -681,8 +695,8 @@ int qmcrt_heliostat_facets(qmcrt_scene* s, int id, float* origins, float* normal
     DBuf o, n;
     o.alloc(std::max<size_t>(t.num_facets, 1) * sizeof(float3));
     n.alloc(std::max<size_t>(t.num_facets, 1) * sizeof(float3));
-    cudaError_t e = s->exact ? qm::launch_facets_exact(t, o.as<float3>(), n.as<float3>(), 0)
-                             : qm::launch_facets_fast(t, o.as<float3>(), n.as<float3>(), 0);
+    cudaError_t e = s->exact == 1 ? qm::launch_facets_exact(t, o.as<float3>(), n.as<float3>(), 0)
+                                  : qm::launch_facets_fast(t, o.as<float3>(), n.as<float3>(), 0);
     cuda_check(e, "facets kernel");
     cuda_check(cudaMemcpy(origins, o.p, (size_t)t.num_facets * sizeof(float3), cudaMemcpyDeviceToHost), "readback");
     cuda_check(cudaMemcpy(normals, n.p, (size_t)t.num_facets * sizeof(float3), cudaMemcpyDeviceToHost), "readback");
@@ -776,7 +790,10 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* s, unsigned seed) {
 }
 
 int qmcrt_set_math_mode(qmcrt_scene* s, int exact) {
-  return guarded([&] { checked(s)->exact = exact ? 1 : 0; });
+  return guarded([&] {
+    if (exact < 0 || exact > 2) invalid("math mode must be 0 (production), 1 (exact) or 2 (production, 48 registers)");
+    checked(s)->exact = exact;
+  });
 }
 
 int qmcrt_set_light_range(qmcrt_scene* s, int begin, int end) {

@@ -70,9 +70,9 @@ struct TraceParams {
   const DevGrid* grids;
   const DevReceiver* receivers;
   const DevTask* tasks;
-  const long long* facet_prefix;  // num_tasks + 1
+  const long long* facet_prefix;  // num_tasks + 1 prefix sums of warp chunks per task
   int num_tasks;
-  long long total_facets;
+  long long total_facets;         // total warp chunks of the launch
   const float4* samples;          // sun-shape pool, P entries (xyz used)
   const float4* perturbations;    // slope-error pool, P entries
   int pool_size;

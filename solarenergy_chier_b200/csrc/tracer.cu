@@ -54,6 +54,23 @@ __device__ __forceinline__ bool eq_eps(float a, float b) {
 }
 __device__ __forceinline__ bool lt_eps(float a, float b) { return (double)a < (double)b - kEps; }
 
+// Where a - b lies relative to +-1e-5, decided in float when the float
+// difference is far enough from both thresholds that its rounding error
+// (at most 2^-24 max(|a|,|b|)) cannot change the answer; kUnsure otherwise
+// (and for NaN), in which case the caller falls back to the double
+// comparisons above.  When it decides, it agrees with them exactly.
+enum EpsOrder { kLess = 0, kTied = 1, kGreater = 2, kUnsure = 3 };
+__device__ __forceinline__ int eps_order(float a, float b) {
+  const float d = a - b;
+  const float m = fmaxf(fabsf(a), fabsf(b)) * 1.2e-7f + 1e-30f;
+  const float e = 1.0e-5f;
+  const float slack = 2.0e-12f;  // covers the float rounding of the 1e-5 constant
+  if (d + m < -e - slack) return kLess;
+  if (d - m > e + slack) return kGreater;
+  if (fabsf(d) + m < e - slack) return kTied;
+  return kUnsure;
+}
+
 // Conservative slab test against one heliostat's padded box.
 __device__ __forceinline__ void slab(float3 r, float3 d, float4 ax, float& tn, float& tf) {
   float ol = r.x * ax.x + r.y * ax.y + r.z * ax.z;
@@ -82,13 +99,18 @@ __device__ __forceinline__ bool sub_hit(const float4* sv, float3 o, float3 d) {
                            make_float3(p1.z, p1.w, p2.x), t, u, v);
 }
 
-// rectGridDDA::intersect over one cell (rectGridDDA.cu:7-25).
-__device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, float3 o, float3 d) {
+// rectGridDDA::intersect over one cell (rectGridDDA.cu:7-25).  A heliostat
+// spanning several cells of the walk is listed in each; seen0/seen1 hold the
+// last two heliostats this walk tested and missed, whose answer cannot change.
+__device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, float3 o, float3 d, int& seen0,
+                                         int& seen1) {
   int b = __ldg(g.hindex + cell), e = __ldg(g.hindex + cell + 1);
   for (int k = b; k < e; ++k) {
     int h = __ldg(g.hmatch + k);
-    if (h == own) continue;
+    if (h == own || h == seen0 || h == seen1) continue;
     int2 sr = __ldg(g.hsub + h);
+    seen1 = seen0;
+    seen0 = h;
     if (sr.y > 1 && !box_hit(g.bound + 4 * h, o, d)) continue;
     for (int s = sr.x; s < sr.x + sr.y; ++s)
       if (sub_hit(g.subv + 3 * s, o, d)) return true;
@@ -100,7 +122,7 @@ __device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, fl
 // the walk leaves the grid; a walk that stops advancing (an exact tie the
 // reference never leaves) or exceeds cells.x+cells.y+cells.z+2 steps ends
 // here with "no hit" and a diagnostic count instead.
-__device__ bool collide(const DevGrid& g, int own, float3 o, float3 d, unsigned& flags) {
+__device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, float3 d, unsigned& flags) {
   float3 rel = make_float3(o.x - g.pos.x, o.y - g.pos.y, o.z - g.pos.z);
   int3 c = trunc3(cdiv(rel, g.interval));
   int3 st = make_int3(d.x >= 0 ? 1 : -1, d.y >= 0 ? 1 : -1, d.z >= 0 ? 1 : -1);
@@ -111,12 +133,28 @@ __device__ bool collide(const DevGrid& g, int own, float3 o, float3 d, unsigned&
   td.x = abs_divide(g.interval.x, d.x);
   td.y = abs_divide(g.interval.y, d.y);
   td.z = abs_divide(g.interval.z, d.z);
+  int seen0 = -1, seen1 = -1;
   for (int it = 0; it < g.max_steps; ++it) {
     if (c.x < 0 || c.x >= g.cells.x || c.y < 0 || c.y >= g.cells.y || c.z < 0 || c.z >= g.cells.z) return false;
     int cell = c.x * g.cells.y * g.cells.z + c.y * g.cells.z + c.z;
-    if (cell_hit(g, cell, own, o, d)) return true;
+    if (cell_hit(g, cell, own, o, d, seen0, seen1)) return true;
     bool sx = false, sy = false, sz = false;
-    if (lt_eps(tm.x, tm.y)) {
+    const int xy = eps_order(tm.x, tm.y);
+    const int xz = eps_order(tm.x, tm.z);
+    const int yz = eps_order(tm.y, tm.z);
+    if (xy != kUnsure && xz != kUnsure && yz != kUnsure) {
+      // less(a,b) <=> kLess, equal(a,b) <=> kTied, less(b,a) <=> kGreater
+      if (xy == kLess) {
+        if (xz != kGreater) { c.x += st.x; sx = true; }
+        if (xz != kLess) { c.z += st.z; sz = true; }
+      } else if (xy == kGreater) {
+        if (yz != kGreater) { c.y += st.y; sy = true; }
+        if (yz != kLess) { c.z += st.z; sz = true; }
+      } else {
+        if (xz != kGreater) { c.x += st.x; c.y += st.y; sx = sy = true; }
+        if (xz != kLess) { c.z += st.z; sz = true; }
+      }
+    } else if (lt_eps(tm.x, tm.y)) {
       if (lt_eps(tm.x, tm.z) || eq_eps(tm.x, tm.z)) { c.x += st.x; sx = true; }
       if (lt_eps(tm.z, tm.x) || eq_eps(tm.x, tm.z)) { c.z += st.z; sz = true; }
     } else if (lt_eps(tm.y, tm.x)) {
@@ -218,58 +256,96 @@ __device__ __forceinline__ int find_task(const long long* prefix, int n, long lo
   return lo;
 }
 
+// Rays of one launch: for task t (a heliostat), rays r in [0, F_t * nl) with
+// facet f = r / nl and light l = light_begin + r % nl, nl = lights per facet.
+// Each warp takes one chunk of kChunk consecutive rays of one task (task ray
+// counts are padded to whole chunks, so a chunk never straddles heliostats);
+// lane i handles rays i, i+32, i+64, ... of the chunk.  With nl >= 32 the 32
+// rays of an iteration share a facet; with fewer lights per facet several
+// facets share a warp and no lane idles.  A lane recomputes its facet only
+// when the facet changes.
+constexpr int kChunkIters = 8;
+constexpr int kChunk = 32 * kChunkIters;
+
 template <bool kRecord>
-__global__ void __launch_bounds__(256) trace_kernel(TraceParams p) {
+#ifndef QM_TRACE_MIN_BLOCKS
+#define QM_TRACE_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(256, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
   const int lane = threadIdx.x & 31;
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  int t, f;
+  const int nl = p.light_end - p.light_begin;
+  // Ray indexes within one heliostat fit in int: the host refuses launches
+  // with num_facets * lights >= 2^31.
+  int t, r0, r_end;
   if (kRecord) {
-    if (warp >= (long long)(p.record_facet_end - p.record_facet_begin)) return;
+    const long long span = (long long)(p.record_facet_end - p.record_facet_begin) * nl;
+    if (warp * kChunk >= span) return;
     t = p.record_task;
-    f = p.record_facet_begin + (int)warp;
+    r0 = p.record_facet_begin * nl + (int)warp * kChunk;
+    r_end = p.record_facet_end * nl;
   } else {
-    if (warp >= p.total_facets) return;
+    if (warp >= p.total_facets) return;  // total_facets holds the number of chunks
     t = find_task(p.facet_prefix, p.num_tasks, warp);
-    f = (int)(warp - __ldg(p.facet_prefix + t));
+    r0 = (int)(warp - __ldg(p.facet_prefix + t)) * kChunk;
+    r_end = p.tasks[t].num_facets * nl;
   }
-  const DevTask T = p.tasks[t];
-  const DevGrid G = p.grids[T.grid];
-  const DevReceiver R = p.receivers[T.receiver];
+  // The task stays in global memory (L1-resident): its facet fields are
+  // read again only when a lane moves to a new facet, which keeps them out
+  // of the registers the grid walk needs.
+  const DevTask& T = p.tasks[t];
+  // Grid and receiver descriptors are likewise read where they are used.
+  const DevGrid& G = p.grids[T.grid];
+  const DevReceiver& R = p.receivers[T.receiver];
+  const int own = T.own;
+  const float factor = T.factor;
   const int P = p.pool_size;
-
-  float3 origin, fnormal;
-  facet_geometry(T, f, origin, fnormal);
-  const Frame nframe = qs::make_frame(fnormal, false);
-  const int g0 = __ldg(T.offsets + f);
-  const int g1 = __ldg(T.offsets + (f + 1) % P);
-  Frame sun;
-  sun.u = p.sun.u;
-  sun.n = p.sun.n;
-  sun.v = p.sun.v;
-  sun.identity = p.sun.identity != 0;
 
   unsigned flags = 0;
   double power = 0.0;
   unsigned long long clamped = 0;
-  const int nl = p.light_end - p.light_begin;
-  for (int l = p.light_begin + lane; l < p.light_end; l += 32) {
+  int cf = -1;
+  float3 origin = make_float3(0.f, 0.f, 0.f);
+  Frame nframe;
+  int g0 = 0, g1 = 0;
+  for (int it = 0; it < kChunkIters; ++it) {
+    const int r = r0 + it * 32 + lane;
+    if (r >= r_end) break;
+    const int f = r / nl;
+    const int l = p.light_begin + (r - f * nl);
+    if (f != cf) {
+      float3 fnormal;
+      facet_geometry(T, f, origin, fnormal);
+      nframe = qs::make_frame(fnormal, false);
+      g0 = __ldg(T.offsets + f);
+      g1 = __ldg(T.offsets + (f + 1) % P);
+      cf = f;
+    }
     const int a = (g0 + l) % P;
-    const float3 dir = qs::to_world(sun, xyz(__ldg(p.samples + a)));
+    float3 dir = xyz(__ldg(p.samples + a));
+    if (!p.sun.identity) {
+      Frame sun;
+      sun.u = p.sun.u;
+      sun.n = p.sun.n;
+      sun.v = p.sun.v;
+      sun.identity = false;
+      dir = qs::to_world(sun, dir);
+    }
     int32_t code;
-    if (collide(G, T.own, origin, dir, flags)) {
+    if (collide(G, own, origin, dir, flags)) {
       code = kShadowed;
     } else {
       const int b = (g1 + l) % P;
       float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(p.perturbations + b))));
       float3 rd = qs::normalize(qs::reflect(neg(dir), n));
-      if (collide(G, T.own, origin, rd, flags)) {
+      if (collide(G, own, origin, rd, flags)) {
         code = kBlocked;
       } else {
         float tt, uu, vv;
         if (!receiver_hit(R, origin, rd, tt, uu, vv)) {
           code = kMissed;
         } else {
-          float e = qs::ray_energy(tt, rd, n, T.factor);
+          float e = qs::ray_energy(tt, rd, n, factor);
           int row = int(qm_rn_mul(uu, (float)R.resolution.y));
           int col = int(qm_rn_mul(vv, (float)R.resolution.x));
           if (row >= R.resolution.y || col >= R.resolution.x || row < 0 || col < 0) {
@@ -316,9 +392,13 @@ cudaError_t QM_SYM(launch_facets)(const DevTask& task, float3* origins, float3* 
   return cudaGetLastError();
 }
 
+int QM_SYM(trace_chunk_rays)() { return kChunk; }
+
 cudaError_t QM_SYM(launch_trace)(const TraceParams& p, bool record, cudaStream_t stream) {
   const int threads = 256;
-  const long long warps = record ? (long long)(p.record_facet_end - p.record_facet_begin) : p.total_facets;
+  const long long nl = p.light_end - p.light_begin;
+  const long long warps = record ? ((long long)(p.record_facet_end - p.record_facet_begin) * nl + kChunk - 1) / kChunk
+                                 : p.total_facets;
   if (warps <= 0) return cudaSuccess;
   const long long blocks = (warps + (threads / 32) - 1) / (threads / 32);
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;

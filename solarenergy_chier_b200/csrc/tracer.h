@@ -11,10 +11,17 @@ namespace qm {
 // (every float operation rounded as the CPU oracle rounds it).
 cudaError_t launch_trace_fast(const TraceParams& p, bool record, cudaStream_t stream);
 cudaError_t launch_trace_exact(const TraceParams& p, bool record, cudaStream_t stream);
+// Production build limited to 48 registers (five 256-thread blocks per SM).
+cudaError_t launch_trace_fast4(const TraceParams& p, bool record, cudaStream_t stream);
+// Rays per warp chunk; TraceParams::facet_prefix counts chunks per task.
+int trace_chunk_rays_fast();
+int trace_chunk_rays_exact();
+int trace_chunk_rays_fast4();
 
 // Micro-facet centres and normals of one heliostat, from the same device
 // function the tracer evaluates per facet.
 cudaError_t launch_facets_fast(const DevTask& task, float3* origins, float3* normals, cudaStream_t stream);
 cudaError_t launch_facets_exact(const DevTask& task, float3* origins, float3* normals, cudaStream_t stream);
+cudaError_t launch_facets_fast4(const DevTask& task, float3* origins, float3* normals, cudaStream_t stream);
 
 }  // namespace qm

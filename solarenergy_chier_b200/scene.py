@@ -168,8 +168,10 @@ class Scene:
     def generate_facet_offsets(self, seed: int) -> None:
         check(self._lib.qmcrt_generate_facet_offsets(self._h, int(seed) & 0xFFFFFFFF))
 
-    def set_math_mode(self, exact: bool) -> None:
-        check(self._lib.qmcrt_set_math_mode(self._h, 1 if exact else 0))
+    def set_math_mode(self, exact) -> None:
+        """True/1: exact build; False/0: production build; 2: production, 48 registers."""
+        mode = int(exact) if not isinstance(exact, bool) else (1 if exact else 0)
+        check(self._lib.qmcrt_set_math_mode(self._h, mode))
 
     def set_light_range(self, begin: int, end: int) -> None:
         check(self._lib.qmcrt_set_light_range(self._h, begin, end))
