@@ -59,6 +59,8 @@ def parse_args():
     p.add_argument("--exact", action="store_true", help="time the kernel build without FMA contraction")
     p.add_argument("--mode", type=int, default=None, help="kernel build: 0 production, 1 exact, 2 production/48 regs")
     p.add_argument("--heliostats", type=int, default=0, help="trace only the first N heliostats (profiling)")
+    p.add_argument("--reference-cuda", type=int, default=0, metavar="N",
+                   help="also time the reference's own CUDA tracer on N heliostats spread over the field")
     return p.parse_args()
 
 
@@ -159,6 +161,43 @@ def cpu_baseline(files, seconds: float):
     if out.returncode != 0:
         raise RuntimeError(out.stderr.strip().splitlines()[-1] if out.stderr.strip() else "cpu baseline failed")
     return json.loads(out.stdout.strip().splitlines()[-1])
+
+
+def reference_cuda(files, scene, count: int):
+    """The reference's CUDA tracer on `count` heliostats spread over the field
+    (oracle/ref_gpu_bench.py, own process), and this tracer on the same ones."""
+    import torch
+
+    nh = scene.num_heliostats
+    ids = sorted({int(round(i * (nh - 1) / max(count - 1, 1))) for i in range(count)})
+    try:
+        out = subprocess.run([sys.executable, "-m", "oracle.ref_gpu_bench", str(files.scene), str(files.config),
+                              *map(str, ids)], capture_output=True, text=True, cwd=str(ROOT), timeout=1200)
+        lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+        if not lines:
+            tail = (out.stderr or "").strip().splitlines()[-3:]
+            return {"unavailable": f"reference CUDA run exited {out.returncode}: {' | '.join(tail)}"}
+        ref = json.loads(lines[-1])
+    except Exception as exc:
+        return {"unavailable": f"reference CUDA run failed: {exc}"}
+    if "unavailable" in ref:
+        return ref
+    # this tracer on the same heliostats, all 2048 lights, one launch
+    L = scene.lights_per_group
+    scene.set_light_range(0, L)
+    scene.trace(ids)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    scene.trace(ids)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    ref["this_tracer_ms"] = ms
+    ref["this_tracer_mrays_s"] = ref["rays"] / (ms / 1e3) / 1e6
+    ref["speedup_vs_reference_kernel"] = ref["this_tracer_mrays_s"] / ref["kernel_mrays_s"]
+    ref["speedup_vs_reference_pipeline"] = ref["this_tracer_mrays_s"] / ref["pipeline_mrays_s"]
+    return ref
 
 
 def run_reference(args):
@@ -311,6 +350,8 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps},
                 "roofline": roofline}
+        if args.reference_cuda > 0:
+            line["reference_cuda"] = reference_cuda(files, scene, args.reference_cuda)
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(files, args.cpu_seconds)

@@ -4,6 +4,9 @@ Compiles files of the SolarEnergy_Chier reference tree (read in place from
 /root/reference, never copied) with nvcc, straight from their sources, into
 oracle/_ref/:
 
+  libref_gpu.so    the reference's CUDA build (every source except main.cpp
+                   and its tests) + ref/ref_gpu_shim.cu, for timing its
+                   tracer on the GPU;
   libref_host.so   the reference's host code (scene files, configuration,
                    scene processing, grid cell lists, heliostat geometry,
                    3D-DDA, receiver intersection, energy, heap classes,
@@ -49,6 +52,17 @@ def _json_include() -> Path | None:
         if (cand / "nlohmann" / "json.hpp").exists():
             return cand
     return None
+
+
+GPU_UNITS = HOST_UNITS + [
+    "Scene/SceneProcessor.cu", "Tool/RandomNumberGenerator/RandomGenerator.cu",
+    "Tool/RandomNumberGenerator/RandomGenerator.cpp",
+    "QuasiMonteCarloRayTracing/QuasiMonteCarloRayTracer.cpp",
+    "QuasiMonteCarloRayTracing/RectangleReceiverRectangleGridRayTracing.cu",
+    "QuasiMonteCarloRayTracing/CylinderReceiverRectangleGridRayTracing.cu",
+    "QuasiMonteCarloRayTracing/Receiver/rectangleReceiverIntersection.cu",
+    "QuasiMonteCarloRayTracing/Receiver/cylinderReceiverIntersection.cu",
+]
 
 
 def include_flags() -> list[str]:
@@ -98,5 +112,40 @@ def build(force: bool = False) -> Path | None:
     return lib
 
 
+def build_gpu(force: bool = False) -> Path | None:
+    """libref_gpu.so: the reference's CUDA code as its own build would run it
+    (-O3, sm_100a, relocatable device code, real CUDA runtime and cuRAND),
+    plus ref/ref_gpu_shim.cu.  Used by bench.py to time the reference tracer."""
+    lib = OUT / "libref_gpu.so"
+    if not available():
+        return lib if lib.exists() else None
+    units = sorted(set(GPU_UNITS))
+    sources = [REF / u for u in units] + [HERE / "ref" / "ref_gpu_shim.cu"]
+    if not force and lib.exists() and all(lib.stat().st_mtime >= s.stat().st_mtime for s in sources):
+        return lib
+    obj_dir = OUT / "obj_gpu"
+    obj_dir.mkdir(parents=True, exist_ok=True)
+    common = ["-O3", "-std=c++14", "-rdc=true", "-Xcompiler", "-fPIC", "-w",
+              "-gencode", "arch=compute_100a,code=sm_100a"] + include_flags()
+    objs = []
+    for src in sources:
+        obj = obj_dir / (src.stem + "_" + src.suffix[1:] + ".o")
+        lang = ["-x", "cu"]
+        cmd = [NVCC, *common, *lang, "-c", str(src), "-o", str(obj)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"reference GPU build failed on {src}")
+        objs.append(str(obj))
+    link = [NVCC, "-shared", "-rdc=true", "-gencode", "arch=compute_100a,code=sm_100a", "--cudart", "static",
+            "-o", str(lib), *objs, "-lcurand"]
+    r = subprocess.run(link, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("reference GPU link failed")
+    return lib
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv))
+    print(build_gpu(force="--force" in sys.argv))

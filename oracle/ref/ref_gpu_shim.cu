@@ -1,0 +1,180 @@
+// CPU ORACLE HARNESS - test/benchmark infrastructure only.
+//
+// C entry points over the reference's own CUDA build (every .cu/.cpp of the
+// reference tree except main.cpp and its tests, compiled by
+// oracle/build_ref.py into oracle/_ref/libref_gpu.so with the real CUDA
+// runtime and cuRAND).  bench.py uses it to time the reference's tracer on
+// the same B200: QuasiMonteCarloRayTracer::rayTracing per heliostat, end to
+// end (B1), and the map_raytracing launch alone (B2).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#define private public
+#define protected public
+#include "CylinderReceiver.cuh"
+#include "CylinderReceiverRectangleGridRayTracing.cuh"
+#include "QuasiMonteCarloRayTracer.h"
+#include "RectangleGrid.cuh"
+#include "RectangleReceiver.cuh"
+#include "RectangleReceiverRectangleGridRayTracing.cuh"
+#include "SceneConfiguration.h"
+#include "SceneLoader.h"
+#include "SceneProcessor.h"
+#include "SolarScene.h"
+#undef private
+#undef protected
+
+namespace {
+std::string g_err;
+bool g_loaded = false;
+}  // namespace
+
+extern "C" {
+
+const char* refgpu_last_error() { return g_err.c_str(); }
+
+// Configuration + scene + SceneProcessor::processScene (cuRAND pools on the GPU).
+int refgpu_load(const char* scene_path, const char* config_path, int* counts3) {
+  if (g_loaded) {
+    g_err = "the reference's singletons hold one scene per process";
+    return -3;
+  }
+  try {
+    SceneConfiguration* cfg = SceneConfiguration::getInstance();
+    cfg->loadConfiguration(config_path);
+    SolarScene* s = SolarScene::GetInstance();
+    SceneLoader loader;
+    if (!loader.SceneFileRead(s, scene_path)) {
+      g_err = "SceneFileRead failed";
+      return -2;
+    }
+    SceneProcessor proc(cfg);
+    if (!proc.processScene(s)) {
+      g_err = "processScene failed";
+      return -2;
+    }
+    counts3[0] = (int)s->getReceivers().size();
+    counts3[1] = (int)s->getGrids().size();
+    counts3[2] = (int)s->getHeliostats().size();
+    g_loaded = true;
+    return 0;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// QuasiMonteCarloRayTracer::rayTracing for each listed heliostat, unchanged
+// (its own cuRAND facet offsets, per-heliostat allocations and syncs); the
+// device time of the whole loop in ms.
+int refgpu_trace_pipeline(const int* ids, int n, float* ms) {
+  try {
+    SolarScene* s = SolarScene::GetInstance();
+    QuasiMonteCarloRayTracer tracer;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaDeviceSynchronize();
+    cudaEventRecord(a);
+    for (int i = 0; i < n; ++i) tracer.rayTracing(s, ids[i]);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return cudaGetLastError() == cudaSuccess ? 0 : -4;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// The tracing launch alone: for each heliostat the reference's arguments are
+// prepared (vertex table, micro-facets, offsets) outside the timed region,
+// then only Rectangle/CylinderReceiverRectangleGridRayTracing is timed.
+// Total kernel ms over the listed heliostats.
+int refgpu_trace_kernels(const int* ids, int n, float* ms) {
+  try {
+    SolarScene* s = SolarScene::GetInstance();
+    QuasiMonteCarloRayTracer tracer;
+    Sunray* sun = s->getSunray();
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float total = 0.0f;
+    for (int i = 0; i < n; ++i) {
+      const int id = ids[i];
+      Heliostat* h = s->getHeliostats()[id];
+      Grid* grid = s->getGrids()[h->getBelongingGridId()];
+      Receiver* recv = s->getReceivers()[grid->getBelongingReceiverIndex()];
+      float3* verts = nullptr;
+      tracer.setFlatRectangleHeliostatVertexs(verts, s->getHeliostats(), grid->getStartHeliostatIndex(),
+                                              grid->getStartHeliostatIndex() + grid->getNumberOfHeliostats());
+      SunrayArgument sa = tracer.generateSunrayArgument(sun);
+      HeliostatArgument ha = tracer.generateHeliostatArgument(s, id);
+      float ratio = h->getPixelLength() / recv->getPixelLength();
+      float factor = sun->getDNI() * ratio * ratio * sun->getReflectiveRate() / float(sun->getNumOfSunshapeLightsPerGroup());
+      cudaDeviceSynchronize();
+      cudaEventRecord(a);
+      if (recv->getType() == 0)
+        RectangleReceiverRectangleGridRayTracing(sa, dynamic_cast<RectangleReceiver*>(recv),
+                                                 dynamic_cast<RectangleGrid*>(grid), ha, verts, factor);
+      else
+        CylinderReceiverRectangleGridRayTracing(sa, dynamic_cast<CylinderReceiver*>(recv),
+                                                dynamic_cast<RectangleGrid*>(grid), ha, verts, factor);
+      cudaEventRecord(b);
+      cudaEventSynchronize(b);
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, a, b);
+      total += t;
+      cudaFree(verts);
+      ha.CClear();
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms = total;
+    return cudaGetLastError() == cudaSuccess ? 0 : -4;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+// Number of micro-facets of a heliostat: the host-side lattice arithmetic
+// that opens CGetDiscreteMicroHelioOriginsAndNormals (RectangleHelio.cu:84-104,
+// FocusFlatRectangleHelio.cu:68-82), without launching its kernels (the
+// focus-flat ones read device frames that only exist after
+// CGetSubHeliostatVertexes).
+int refgpu_num_facets(int id) {
+  Heliostat* h = SolarScene::GetInstance()->getHeliostats()[id];
+  int2 rc = h->getRowAndColumn();
+  float3 size = h->getSize();
+  float2 gap = h->getGap();
+  float lx = (size.z - gap.y * (rc.x - 1)) / float(rc.x);
+  float ly = (size.x - gap.x * (rc.y - 1)) / float(rc.y);
+  int sx = int(lx / h->getPixelLength());
+  int sy = int(ly / h->getPixelLength());
+  return rc.x * rc.y * sx * sy;
+}
+
+int refgpu_lights_per_group() { return SolarScene::GetInstance()->getSunray()->getNumOfSunshapeLightsPerGroup(); }
+
+int refgpu_pool_size() {
+  Sunray* sun = SolarScene::GetInstance()->getSunray();
+  return sun->getNumOfSunshapeGroups() * sun->getNumOfSunshapeLightsPerGroup();
+}
+
+// Receiver image read-back (float, rows x cols).
+int refgpu_image(int r, float* out, int* w, int* h) {
+  Receiver* recv = SolarScene::GetInstance()->getReceivers()[r];
+  *w = recv->getResolution().x;
+  *h = recv->getResolution().y;
+  if (out) cudaMemcpy(out, recv->getDeviceImage(), sizeof(float) * (*w) * (*h), cudaMemcpyDeviceToHost);
+  return 0;
+}
+
+}  // extern "C"
