@@ -324,12 +324,20 @@ def main():
         per_ray = census(files)
         fp32_peak = fp32_peak_tflops(torch)
         achieved_tflops = value * 1e6 * per_ray["flops"] / 1e12
+        from solarenergy_chier_b200 import microbench
+
+        atom_rate = microbench.l2_atomics_per_s(scene.receiver(0)["width"] * scene.receiver(0)["height"])
+        fp32_ceiling = fp32_peak * 1e12 / per_ray["flops"]
+        atom_ceiling = atom_rate / max(per_ray["hit"], 1e-12)
         roofline = {"bound": "fp32", "achieved": achieved_tflops, "peak": fp32_peak, "unit": "TFLOP/s",
                     "frac": achieved_tflops / fp32_peak if fp32_peak else None,
                     "traffic": None,
                     "peak_source": "measured in bench.py: non-tensor FP32 FMA microbenchmark on this GPU "
                                    "(MEASURED_PEAKS.json holds no non-tensor FP32 figure)",
                     "flops_per_ray": per_ray["flops"], "work_per_ray": per_ray,
+                    "ceiling_mrays_s": {"fp32": fp32_ceiling / 1e6, "l2_atomics": atom_ceiling / 1e6,
+                                        "binding": "fp32" if fp32_ceiling <= atom_ceiling else "l2_atomics"},
+                    "l2_atomics_per_s": atom_rate,
                     "kernel_ms_per_step": kernel_ms_max / args.steps}
         prof = ROOT / "profiles" / "trace_kernel_traffic.json"
         if prof.exists():

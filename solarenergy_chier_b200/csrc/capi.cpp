@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -173,67 +174,152 @@ using qm::DevGrid;
 using qm::DevReceiver;
 using qm::DevTask;
 
-// Padded bounding box of one heliostat in its own frame, from the corners of
-// all its sub-heliostat parallelograms (double precision, then widened).
-void heliostat_box(const qm::HeliostatModel& h, const std::vector<float3>& verts, float4 out[4]) {
-  double n[3] = {h.normal.x, h.normal.y, h.normal.z};
-  double nl = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
-  if (!(nl > 0)) {
-    n[0] = 0;
-    n[1] = 1;
-    n[2] = 0;
-    nl = 1;
+// Traversal record of one heliostat: a padded bounding box in a frame
+// aligned with its sub-heliostat lattice, and the lattice itself, so that a
+// ray entering the box only tests the sub-heliostats under its path.
+//
+// Frame: ex along the summed column edges (vertex A -> C of every
+// sub-heliostat), ez along the summed row edges (A -> B) made orthogonal to
+// ex, and their normal.  Box: the extent of every sub-heliostat corner along
+// the three axes, widened by `margin` (1 cm plus 1e-5 of the coordinate
+// scale, far above the float rounding of the box and parallelogram tests).
+//
+// Lattice: column c of the heliostat is assigned the band
+// [x0 + c px, x0 + (c+1) px] along ex, row r the band [z0 + r pz, z0 + (r+1) pz]
+// along ez (bands fitted to the column and row extents, gap-centred).  The
+// slack is the largest distance by which any corner of a sub-heliostat leaves
+// its band; the window margin is margin + slack.  A ray hitting sub-heliostat
+// (r, c) does so at a point whose ex coordinate lies in column c's band
+// widened by the window margin and inside the ray's own ex range within the
+// box, so the columns whose widened band meets that range (and likewise the
+// rows) hold every sub-heliostat the ray can hit, whatever the geometry: an
+// irregular layout only widens the window.  Degenerate frames fall back to a
+// window covering every sub-heliostat.
+//
+// Output (5 float4): centre.xyz + window margin; (ex, half_x); (n, half_n);
+// (ez, half_z); (x0, 1/px, z0, 1/pz).  rows_cols receives the lattice shape
+// (rows * cols == num_sub).
+void heliostat_box(const qm::HeliostatModel& h, const std::vector<float3>& verts, float4 out[5], int2& rows_cols) {
+  using D3 = std::array<double, 3>;
+  auto dot = [](const D3& a, const D3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+  auto unit = [&](D3& a) {
+    double l = std::sqrt(dot(a, a));
+    if (!(l > 0) || !std::isfinite(l)) return false;
+    for (double& x : a) x /= l;
+    return true;
+  };
+  auto cross = [](const D3& a, const D3& b) {
+    return D3{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+  };
+  const int ns = h.num_sub;
+  int rows = h.row_col.x, cols = h.row_col.y;
+  bool lattice = ns > 1 && rows > 0 && cols > 0 && rows * cols == ns;
+  if (!lattice) {
+    rows = 1;
+    cols = std::max(ns, 1);
   }
-  for (double& x : n) x /= nl;
-  double e1[3];
-  if (std::fabs(n[0]) < 0.9) {
-    // e1 = normalize(cross((1,0,0), n))
-    e1[0] = 0;
-    e1[1] = -n[2];
-    e1[2] = n[1];
-  } else {
-    // e1 = normalize(cross((0,0,1), n))
-    e1[0] = -n[1];
-    e1[1] = n[0];
-    e1[2] = 0;
-  }
-  double l1 = std::sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
-  for (double& x : e1) x /= l1;
-  double e3[3] = {e1[1] * n[2] - e1[2] * n[1], e1[2] * n[0] - e1[0] * n[2], e1[0] * n[1] - e1[1] * n[0]};
-  const double* ax[3] = {e1, n, e3};
-  const double c0[3] = {h.pos.x, h.pos.y, h.pos.z};
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  double maxabs = std::fabs(c0[0]) + std::fabs(c0[1]) + std::fabs(c0[2]);
-  for (int s = h.sub_begin; s < h.sub_begin + h.num_sub; ++s) {
+  std::vector<std::array<D3, 4>> corners(ns);
+  D3 sx{0, 0, 0}, sz{0, 0, 0};
+  for (int k = 0; k < ns; ++k) {
+    const int s = h.sub_begin + k;
     const float3 B = verts[3 * s], A = verts[3 * s + 1], C = verts[3 * s + 2];
-    const double a[3] = {A.x, A.y, A.z};
-    const double ab[3] = {(double)B.x - A.x, (double)B.y - A.y, (double)B.z - A.z};
-    const double ac[3] = {(double)C.x - A.x, (double)C.y - A.y, (double)C.z - A.z};
-    for (int corner = 0; corner < 4; ++corner) {
-      double p[3];
+    const D3 a{A.x, A.y, A.z};
+    const D3 ab{(double)B.x - A.x, (double)B.y - A.y, (double)B.z - A.z};
+    const D3 ac{(double)C.x - A.x, (double)C.y - A.y, (double)C.z - A.z};
+    for (int corner = 0; corner < 4; ++corner)
       for (int i = 0; i < 3; ++i)
-        p[i] = a[i] + ((corner & 1) ? ab[i] : 0.0) + ((corner & 2) ? ac[i] : 0.0) - c0[i];
-      for (int k = 0; k < 3; ++k) {
-        double d = p[0] * ax[k][0] + p[1] * ax[k][1] + p[2] * ax[k][2];
-        lo[k] = std::min(lo[k], d);
-        hi[k] = std::max(hi[k], d);
-      }
-      maxabs = std::max(maxabs, std::fabs(p[0] + c0[0]) + std::fabs(p[1] + c0[1]) + std::fabs(p[2] + c0[2]));
+        corners[k][corner][i] = a[i] + ((corner & 1) ? ab[i] : 0.0) + ((corner & 2) ? ac[i] : 0.0);
+    for (int i = 0; i < 3; ++i) {
+      sx[i] += ac[i];
+      sz[i] += ab[i];
     }
   }
-  // Padding: 1 cm plus 1e-5 of the coordinate scale, two orders of magnitude
-  // above the float rounding of the parallelogram test at that scale.
-  const double margin = 0.01 + 1e-5 * maxabs;
-  double centre[3] = {c0[0], c0[1], c0[2]};
-  double half[3];
-  for (int k = 0; k < 3; ++k) {
-    double mid = 0.5 * (lo[k] + hi[k]);
-    for (int i = 0; i < 3; ++i) centre[i] += mid * ax[k][i];
-    half[k] = 0.5 * (hi[k] - lo[k]) + margin;
+  D3 ex = sx, ez = sz, n{0, 0, 0};
+  bool frame = unit(ex);
+  if (frame) {
+    const double p = dot(ez, ex);
+    for (int i = 0; i < 3; ++i) ez[i] -= p * ex[i];
+    frame = unit(ez);
   }
-  out[0] = make_float4((float)centre[0], (float)centre[1], (float)centre[2], 0.0f);
-  for (int k = 0; k < 3; ++k)
-    out[1 + k] = make_float4((float)ax[k][0], (float)ax[k][1], (float)ax[k][2], (float)(half[k] * (1 + 1e-6)));
+  if (frame) {
+    n = cross(ez, ex);
+    frame = unit(n);
+  }
+  if (!frame) {
+    // Any orthonormal frame around the heliostat normal; no lattice.
+    n = D3{h.normal.x, h.normal.y, h.normal.z};
+    if (!unit(n)) n = D3{0, 1, 0};
+    ex = std::fabs(n[0]) < 0.9 ? D3{0, -n[2], n[1]} : D3{-n[1], n[0], 0};
+    unit(ex);
+    ez = cross(ex, n);
+    lattice = false;
+    rows = 1;
+    cols = std::max(ns, 1);
+  }
+  const D3* ax[3] = {&ex, &n, &ez};
+  const D3 c0{h.pos.x, h.pos.y, h.pos.z};
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  double maxabs = std::fabs(c0[0]) + std::fabs(c0[1]) + std::fabs(c0[2]);
+  for (int k = 0; k < ns; ++k)
+    for (const D3& q : corners[k]) {
+      const D3 p{q[0] - c0[0], q[1] - c0[1], q[2] - c0[2]};
+      for (int a = 0; a < 3; ++a) {
+        const double d = dot(p, *ax[a]);
+        lo[a] = std::min(lo[a], d);
+        hi[a] = std::max(hi[a], d);
+      }
+      maxabs = std::max(maxabs, std::fabs(q[0]) + std::fabs(q[1]) + std::fabs(q[2]));
+    }
+  const double margin = 0.01 + 1e-5 * maxabs;
+  D3 centre = c0;
+  double half[3];
+  for (int a = 0; a < 3; ++a) {
+    const double mid = 0.5 * (lo[a] + hi[a]);
+    for (int i = 0; i < 3; ++i) centre[i] += mid * (*ax[a])[i];
+    half[a] = 0.5 * (hi[a] - lo[a]) + margin;
+  }
+  // Lattice bands in box-centre coordinates.
+  double x0 = 0, px = 1, z0 = 0, pz = 1, slack = 0;
+  if (lattice) {
+    std::vector<double> xl(cols, 1e300), xh(cols, -1e300), zl(rows, 1e300), zh(rows, -1e300);
+    for (int k = 0; k < ns; ++k) {
+      const int r = k / cols, c = k % cols;
+      for (const D3& q : corners[k]) {
+        const D3 p{q[0] - centre[0], q[1] - centre[1], q[2] - centre[2]};
+        const double x = dot(p, ex), z = dot(p, ez);
+        xl[c] = std::min(xl[c], x);
+        xh[c] = std::max(xh[c], x);
+        zl[r] = std::min(zl[r], z);
+        zh[r] = std::max(zh[r], z);
+      }
+    }
+    auto fit = [&](const std::vector<double>& l, const std::vector<double>& u, double& b0, double& pitch) {
+      const int m = (int)l.size();
+      double gap = 0;
+      for (int i = 0; i + 1 < m; ++i) gap += l[i + 1] - u[i];
+      gap = m > 1 ? gap / (m - 1) : 0.0;
+      pitch = (u[m - 1] - l[0] + gap) / m;
+      b0 = l[0] - 0.5 * gap;
+      if (!(pitch > 0) || !std::isfinite(pitch)) return false;
+      for (int i = 0; i < m; ++i) {
+        slack = std::max(slack, (b0 + i * pitch) - l[i]);
+        slack = std::max(slack, u[i] - (b0 + (i + 1) * pitch));
+      }
+      return true;
+    };
+    lattice = fit(xl, xh, x0, px) && fit(zl, zh, z0, pz) && std::isfinite(slack);
+  }
+  const double window = lattice ? margin + slack : 1e30;
+  if (!lattice) {
+    x0 = z0 = 0;
+    px = pz = 1;
+  }
+  out[0] = make_float4((float)centre[0], (float)centre[1], (float)centre[2], (float)window);
+  for (int a = 0; a < 3; ++a)
+    out[1 + a] = make_float4((float)(*ax[a])[0], (float)(*ax[a])[1], (float)(*ax[a])[2], (float)(half[a] * (1 + 1e-6)));
+  // A single column (row) maps every x (z) to band 0.
+  out[4] = make_float4((float)x0, cols > 1 ? (float)(1.0 / px) : 0.0f, (float)z0, rows > 1 ? (float)(1.0 / pz) : 0.0f);
+  rows_cols = make_int2(rows, cols);
 }
 
 void build_device_scene(qmcrt_scene* s) {
@@ -253,12 +339,13 @@ void build_device_scene(qmcrt_scene* s) {
     auto gb = std::make_unique<GridBufs>();
     upload(gb->hindex, g.cell_hindex);
     upload(gb->hmatch, g.cell_hmatch);
-    std::vector<float4> bound(4 * (size_t)g.num_heliostats);
-    std::vector<int2> hsub(g.num_heliostats);
+    std::vector<float4> bound(5 * (size_t)g.num_heliostats);
+    std::vector<int4> hsub(g.num_heliostats);
     for (int i = 0; i < g.num_heliostats; ++i) {
       const qm::HeliostatModel& h = m.heliostats[g.start_heliostat + i];
-      hsub[i] = make_int2(h.sub_begin, h.num_sub);
-      heliostat_box(h, g.sub_vertices, &bound[4 * (size_t)i]);
+      int2 rc;
+      heliostat_box(h, g.sub_vertices, &bound[5 * (size_t)i], rc);
+      hsub[i] = make_int4(h.sub_begin, h.num_sub, rc.x, rc.y);
     }
     upload(gb->bound, bound);
     upload(gb->hsub, hsub);
@@ -279,7 +366,7 @@ void build_device_scene(qmcrt_scene* s) {
     dg.hindex = gb->hindex.as<int>();
     dg.hmatch = gb->hmatch.as<int>();
     dg.bound = gb->bound.as<float4>();
-    dg.hsub = gb->hsub.as<int2>();
+    dg.hsub = gb->hsub.as<int4>();
     dg.subv = gb->subv.as<float4>();
     s->grids.push_back(dg);
     s->grid_bufs.push_back(std::move(gb));
@@ -482,13 +569,17 @@ cudaError_t run_trace(qmcrt_scene* s, const qm::TraceParams& p, bool record, cud
   }
 }
 
+// Rays of one heliostat in one launch: the kernel indexes them with int,
+// with 2^16 of headroom for a warp's chunk past the end.
+constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;
+
 void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
   if (n < 0 || (n > 0 && !ids)) invalid("heliostat list is invalid");
   for (int i = 0; i < n; ++i) check_heliostat(s, ids[i]);
   if (n == 0) return;
   for (int i = 0; i < n; ++i)
-    if ((long long)s->templates[ids[i]].num_facets * (s->light_end - s->light_begin) >= 0x7fffffffLL)
-      invalid("a heliostat's micro-facets x lights must stay below 2^31 rays per launch; trace fewer lights");
+    if ((long long)s->templates[ids[i]].num_facets * (s->light_end - s->light_begin) > kMaxTaskRays)
+      invalid("a heliostat's micro-facets x lights must stay below 2^31 - 2^16 rays per launch; trace fewer lights");
   DeviceGuard guard(s->device);
   const long long nl = s->light_end - s->light_begin;
   if (nl == 0) return;
@@ -903,6 +994,7 @@ int qmcrt_debug_hit_records(qmcrt_scene* s, int id, int fb, int fe, int lb, int 
     if (fb < 0 || fe < fb || fe > nf) invalid("facet range out of bounds");
     if (lb < 0 || le < lb || le > s->model.config.num_per_sunshape_group) invalid("light range out of bounds");
     if (!codes) invalid("output is NULL");
+    if ((long long)fe * (le - lb) > kMaxTaskRays) invalid("facet_end x lights must stay below 2^31 - 2^16");
     const size_t count = (size_t)(fe - fb) * (le - lb);
     if (count == 0) return;
     DeviceGuard guard(s->device);

@@ -16,8 +16,9 @@ struct DevGrid {
   int max_steps;        // DDA step bound: cells.x + cells.y + cells.z + 2
   const int* hindex;    // heliostat-level CSR offsets, cells + 1 entries
   const int* hmatch;    // grid-local heliostat ids per cell
-  const float4* bound;  // 4 float4 per grid-local heliostat: centre, then (axis_k, half extent_k)
-  const int2* hsub;     // (first sub-heliostat id, sub-heliostat count) per grid-local heliostat
+  const float4* bound;  // 5 float4 per grid-local heliostat: (centre, window margin), (axis_k, half extent_k)
+                        // for k = lattice x, normal, lattice z, then (x0, 1/px, z0, 1/pz)
+  const int4* hsub;     // (first sub-heliostat id, count, lattice rows, lattice columns) per grid-local heliostat
   const float4* subv;   // 3 float4 per sub-heliostat: A.xyz AB.x | AB.yz AC.xy | AC.z
 };
 
@@ -77,6 +78,7 @@ struct TraceParams {
   const float4* perturbations;    // slope-error pool, P entries
   int pool_size;
   int light_begin, light_end;     // light indexes traced per facet
+  int lights_q32, lights_r32;     // 32 / (light_end - light_begin) and 32 % it (set by the launcher)
   SunFrame sun;                   // frame of -sun_dir
   double* power;                  // FP64 per-slot power accumulators
   unsigned long long* diag;

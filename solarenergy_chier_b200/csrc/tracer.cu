@@ -13,8 +13,9 @@
 // The walk is the reference's 3D-DDA (QuasiMonteCarloRayTracing/Grid/rectGridDDA.cu:31-119)
 // step for step, including its 1e-5 tie rules and truncating start cell.
 // Inside a cell each heliostat is first tested against a padded bounding
-// box in its own frame; only boxes the ray enters have their sub-heliostat
-// parallelograms tested.  The box is conservative (padding far above float
+// box aligned with its sub-heliostat lattice; a ray entering the box tests
+// only the sub-heliostats of the lattice rows and columns its path inside
+// the box crosses.  Box and window are conservative (padding far above float
 // rounding) so the any-hit answer is unchanged.
 //
 // Everything outside the grid walk (sampling, facet geometry, slope error,
@@ -71,25 +72,52 @@ __device__ __forceinline__ int eps_order(float a, float b) {
   return kUnsure;
 }
 
-// Conservative slab test against one heliostat's padded box.
-__device__ __forceinline__ void slab(float3 r, float3 d, float4 ax, float& tn, float& tf) {
-  float ol = r.x * ax.x + r.y * ax.y + r.z * ax.z;
-  float dl = d.x * ax.x + d.y * ax.y + d.z * ax.z;
-  float inv = __fdividef(1.0f, dl);
-  float t0 = (-ax.w - ol) * inv;
-  float t1 = (ax.w - ol) * inv;
+// Conservative slab test along one axis of a heliostat's padded box; ol and
+// dl are the ray origin (relative to the box centre) and direction along it.
+__device__ __forceinline__ void slab(float ol, float dl, float half, float& tn, float& tf) {
+  const float inv = __fdividef(1.0f, dl);
+  const float t0 = (-half - ol) * inv;
+  const float t1 = (half - ol) * inv;
   tn = fmaxf(tn, fminf(t0, t1));
   tf = fminf(tf, fmaxf(t0, t1));
 }
 
-__device__ __forceinline__ bool box_hit(const float4* b, float3 o, float3 d) {
-  float4 c = __ldg(b);
-  float3 r = make_float3(o.x - c.x, o.y - c.y, o.z - c.z);
+__device__ __forceinline__ int band(float x, float inv_pitch, int n) {
+  return (int)fminf(fmaxf(floorf(x * inv_pitch), 0.0f), (float)(n - 1));
+}
+
+// The ray against one heliostat's traversal record (5 float4, built by the
+// host): false if it misses the padded box, else the window of lattice rows
+// [r0, r1] and columns [c0, c1] holding every sub-heliostat it can hit --
+// the lattice bands met by the ray's own extent inside the box, widened by
+// the record's window margin.
+__device__ __forceinline__ bool box_window(const float4* b, int rows, int cols, float3 o, float3 d, int& r0,
+                                           int& r1, int& c0, int& c1) {
+  const float4 c = __ldg(b);
+  const float3 r = make_float3(o.x - c.x, o.y - c.y, o.z - c.z);
+  const float4 an = __ldg(b + 2);
+  const float oln = r.x * an.x + r.y * an.y + r.z * an.z;
+  const float dln = d.x * an.x + d.y * an.y + d.z * an.z;
   float tn = -3.0e38f, tf = 3.0e38f;
-  slab(r, d, __ldg(b + 1), tn, tf);
-  slab(r, d, __ldg(b + 2), tn, tf);
-  slab(r, d, __ldg(b + 3), tn, tf);
-  return tn <= tf && tf >= -1.0f;
+  slab(oln, dln, an.w, tn, tf);
+  const float4 ax = __ldg(b + 1);
+  const float olx = r.x * ax.x + r.y * ax.y + r.z * ax.z;
+  const float dlx = d.x * ax.x + d.y * ax.y + d.z * ax.z;
+  slab(olx, dlx, ax.w, tn, tf);
+  const float4 az = __ldg(b + 3);
+  const float olz = r.x * az.x + r.y * az.y + r.z * az.z;
+  const float dlz = d.x * az.x + d.y * az.y + d.z * az.z;
+  slab(olz, dlz, az.w, tn, tf);
+  if (!(tn <= tf && tf >= -1.0f)) return false;
+  tn = fmaxf(tn, -1.0f);
+  const float4 lat = __ldg(b + 4);  // x0, 1/px, z0, 1/pz
+  const float xa = olx + tn * dlx, xb = olx + tf * dlx;
+  const float za = olz + tn * dlz, zb = olz + tf * dlz;
+  c0 = band(fminf(xa, xb) - c.w - lat.x, lat.y, cols);
+  c1 = band(fmaxf(xa, xb) + c.w - lat.x, lat.y, cols);
+  r0 = band(fminf(za, zb) - c.w - lat.z, lat.w, rows);
+  r1 = band(fmaxf(za, zb) + c.w - lat.z, lat.w, rows);
+  return true;
 }
 
 __device__ __forceinline__ bool sub_hit(const float4* sv, float3 o, float3 d) {
@@ -102,18 +130,27 @@ __device__ __forceinline__ bool sub_hit(const float4* sv, float3 o, float3 d) {
 // rectGridDDA::intersect over one cell (rectGridDDA.cu:7-25).  A heliostat
 // spanning several cells of the walk is listed in each; seen0/seen1 hold the
 // last two heliostats this walk tested and missed, whose answer cannot change.
+// The reference tests every sub-heliostat of every listed heliostat and
+// stops at the first hit; only the answer (hit or not) is used, so testing
+// just the sub-heliostats inside the ray's window gives the same answer.
 __device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, float3 o, float3 d, int& seen0,
                                          int& seen1) {
   int b = __ldg(g.hindex + cell), e = __ldg(g.hindex + cell + 1);
   for (int k = b; k < e; ++k) {
     int h = __ldg(g.hmatch + k);
     if (h == own || h == seen0 || h == seen1) continue;
-    int2 sr = __ldg(g.hsub + h);
+    const int4 hs = __ldg(g.hsub + h);  // first sub-heliostat, count, lattice rows, lattice columns
     seen1 = seen0;
     seen0 = h;
-    if (sr.y > 1 && !box_hit(g.bound + 4 * h, o, d)) continue;
-    for (int s = sr.x; s < sr.x + sr.y; ++s)
-      if (sub_hit(g.subv + 3 * s, o, d)) return true;
+    if (hs.y == 1) {
+      if (sub_hit(g.subv + 3 * hs.x, o, d)) return true;
+      continue;
+    }
+    int r0, r1, c0, c1;
+    if (!box_window(g.bound + 5 * h, hs.z, hs.w, o, d, r0, r1, c0, c1)) continue;
+    for (int rr = r0; rr <= r1; ++rr)
+      for (int cc = c0; cc <= c1; ++cc)
+        if (sub_hit(g.subv + 3 * (hs.x + rr * hs.w + cc), o, d)) return true;
   }
   return false;
 }
@@ -135,10 +172,27 @@ __device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, flo
   td.z = abs_divide(g.interval.z, d.z);
   int seen0 = -1, seen1 = -1;
   for (int it = 0; it < g.max_steps; ++it) {
-    if (c.x < 0 || c.x >= g.cells.x || c.y < 0 || c.y >= g.cells.y || c.z < 0 || c.z >= g.cells.z) return false;
+    if ((unsigned)c.x >= (unsigned)g.cells.x || (unsigned)c.y >= (unsigned)g.cells.y ||
+        (unsigned)c.z >= (unsigned)g.cells.z)
+      return false;
     int cell = c.x * g.cells.y * g.cells.z + c.y * g.cells.z + c.z;
     if (cell_hit(g, cell, own, o, d, seen0, seen1)) return true;
     bool sx = false, sy = false, sz = false;
+    // Common case: one boundary is nearer than both others by more than
+    // 1e-5 plus the float rounding of the difference (tm >= 0, so the error
+    // of tm_j - min is at most 2^-24 tm_j).  The reference's rules then step
+    // that axis alone, whatever the order of the other two.
+    const float mn = fminf(fminf(tm.x, tm.y), tm.z);
+    const float c0 = 1.0e-5f + 2.0e-12f;
+    const bool gx = tm.x - mn > fmaf(tm.x, 1.2e-7f, c0);
+    const bool gy = tm.y - mn > fmaf(tm.y, 1.2e-7f, c0);
+    const bool gz = tm.z - mn > fmaf(tm.z, 1.2e-7f, c0);
+    if ((int)gx + (int)gy + (int)gz == 2) {
+      if (!gx) { c.x += st.x; tm.x += td.x; }
+      else if (!gy) { c.y += st.y; tm.y += td.y; }
+      else { c.z += st.z; tm.z += td.z; }
+      continue;
+    }
     const int xy = eps_order(tm.x, tm.y);
     const int xz = eps_order(tm.x, tm.z);
     const int yz = eps_order(tm.y, tm.z);
@@ -262,17 +316,38 @@ __device__ __forceinline__ int find_task(const long long* prefix, int n, long lo
 // counts are padded to whole chunks, so a chunk never straddles heliostats);
 // lane i handles rays i, i+32, i+64, ... of the chunk.  With nl >= 32 the 32
 // rays of an iteration share a facet; with fewer lights per facet several
-// facets share a warp and no lane idles.  A lane recomputes its facet only
-// when the facet changes.
+// facets share a warp and no lane idles.
+//
+// Facet window: the facets of an iteration lie within 32 consecutive ids
+// (at most ceil(32/nl) + 1 <= 32 of them), so a warp keeps a window of 32
+// facets in shared memory -- origin, normal frame and the two pool offsets --
+// computed one facet per lane, and refills it only when an iteration needs a
+// facet past its end (once per chunk for nl >= 9).  Per-ray work then reads
+// the window instead of re-deriving the facet, and holds no facet state in
+// registers across the grid walks.
 constexpr int kChunkIters = 8;
 constexpr int kChunk = 32 * kChunkIters;
+#ifndef QM_TRACE_THREADS
+#define QM_TRACE_THREADS 256
+#endif
+constexpr int kThreads = QM_TRACE_THREADS;
+constexpr int kWindow = 32;
+
+struct FacetWindow {
+  float4 o[kThreads];  // origin.xyz, pool offset g[f] (int bits)
+  float4 u[kThreads];  // frame u.xyz, pool offset g[(f+1) % P] (int bits)
+  float4 n[kThreads];  // frame n.xyz, frame identity flag
+  float4 v[kThreads];  // frame v.xyz
+};
 
 template <bool kRecord>
 #ifndef QM_TRACE_MIN_BLOCKS
 #define QM_TRACE_MIN_BLOCKS 4
 #endif
-__global__ void __launch_bounds__(256, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
+__global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
+  __shared__ FacetWindow win;
   const int lane = threadIdx.x & 31;
+  const int wbase = threadIdx.x & ~31;  // this warp's 32 window slots
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int nl = p.light_end - p.light_begin;
   // Ray indexes within one heliostat fit in int: the host refuses launches
@@ -290,77 +365,103 @@ __global__ void __launch_bounds__(256, QM_TRACE_MIN_BLOCKS) trace_kernel(TracePa
     r0 = (int)(warp - __ldg(p.facet_prefix + t)) * kChunk;
     r_end = p.tasks[t].num_facets * nl;
   }
-  // The task stays in global memory (L1-resident): its facet fields are
-  // read again only when a lane moves to a new facet, which keeps them out
-  // of the registers the grid walk needs.
+  // The task stays in global memory (L1-resident) and is read where used.
   const DevTask& T = p.tasks[t];
-  // Grid and receiver descriptors are likewise read where they are used.
   const DevGrid& G = p.grids[T.grid];
   const DevReceiver& R = p.receivers[T.receiver];
-  const int own = T.own;
-  const float factor = T.factor;
   const int P = p.pool_size;
+  // This lane's first ray; later rays advance by 32 = q32 * nl + r32.
+  int f = (r0 + lane) / nl;
+  int l = (r0 + lane) - f * nl;
+  const int q32 = p.lights_q32, r32 = p.lights_r32;
+  const int iters = min(kChunkIters, (r_end - r0 + 31) >> 5);  // warp-uniform
 
   unsigned flags = 0;
   double power = 0.0;
   unsigned long long clamped = 0;
-  int cf = -1;
-  float3 origin = make_float3(0.f, 0.f, 0.f);
-  Frame nframe;
-  int g0 = 0, g1 = 0;
-  for (int it = 0; it < kChunkIters; ++it) {
-    const int r = r0 + it * 32 + lane;
-    if (r >= r_end) break;
-    const int f = r / nl;
-    const int l = p.light_begin + (r - f * nl);
-    if (f != cf) {
-      float3 fnormal;
-      facet_geometry(T, f, origin, fnormal);
-      nframe = qs::make_frame(fnormal, false);
-      g0 = __ldg(T.offsets + f);
-      g1 = __ldg(T.offsets + (f + 1) % P);
-      cf = f;
+  int base = 0;        // first facet id of the window
+  bool filled = false;  // warp-uniform
+  for (int it = 0; it < iters; ++it) {
+    const bool active = r0 + it * 32 + lane < r_end;
+    // Lane 0 holds the smallest facet of the iteration (it is active whenever
+    // any lane is) and every facet of the iteration lies within 31 of it.
+    const int f0 = __shfl_sync(0xffffffffu, f, 0);
+    if (__any_sync(0xffffffffu, active && (!filled || f - base >= kWindow))) {
+      __syncwarp();
+      base = f0;
+      filled = true;
+      const int fw = base + lane;
+      if (fw < T.num_facets) {
+        float3 origin, fnormal;
+        facet_geometry(T, fw, origin, fnormal);
+        const Frame fr = qs::make_frame(fnormal, false);
+        win.o[wbase + lane] = make_float4(origin.x, origin.y, origin.z, __int_as_float(__ldg(T.offsets + fw)));
+        win.u[wbase + lane] = make_float4(fr.u.x, fr.u.y, fr.u.z, __int_as_float(__ldg(T.offsets + (fw + 1) % P)));
+        win.n[wbase + lane] = make_float4(fr.n.x, fr.n.y, fr.n.z, fr.identity ? 1.0f : 0.0f);
+        win.v[wbase + lane] = make_float4(fr.v.x, fr.v.y, fr.v.z, 0.0f);
+      }
+      __syncwarp();
     }
-    const int a = (g0 + l) % P;
-    float3 dir = xyz(__ldg(p.samples + a));
-    if (!p.sun.identity) {
-      Frame sun;
-      sun.u = p.sun.u;
-      sun.n = p.sun.n;
-      sun.v = p.sun.v;
-      sun.identity = false;
-      dir = qs::to_world(sun, dir);
-    }
-    int32_t code;
-    if (collide(G, own, origin, dir, flags)) {
-      code = kShadowed;
-    } else {
-      const int b = (g1 + l) % P;
-      float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(p.perturbations + b))));
-      float3 rd = qs::normalize(qs::reflect(neg(dir), n));
-      if (collide(G, own, origin, rd, flags)) {
-        code = kBlocked;
+    if (active) {
+      const int slot = wbase + (f - base);
+      const int lab = p.light_begin + l;
+      // Pool offsets lie in [0, P) and light indexes in [0, L), L <= P.
+      int a = __float_as_int(win.o[slot].w) + lab;
+      a -= a >= P ? P : 0;
+      float3 dir = xyz(__ldg(p.samples + a));
+      if (!p.sun.identity) {
+        Frame sun;
+        sun.u = p.sun.u;
+        sun.n = p.sun.n;
+        sun.v = p.sun.v;
+        sun.identity = false;
+        dir = qs::to_world(sun, dir);
+      }
+      int32_t code;
+      if (collide(G, T.own, xyz(win.o[slot]), dir, flags)) {
+        code = kShadowed;
       } else {
-        float tt, uu, vv;
-        if (!receiver_hit(R, origin, rd, tt, uu, vv)) {
-          code = kMissed;
+        int b = __float_as_int(win.u[slot].w) + lab;
+        b -= b >= P ? P : 0;
+        Frame nframe;
+        nframe.u = xyz(win.u[slot]);
+        const float4 wn = win.n[slot];
+        nframe.n = xyz(wn);
+        nframe.v = xyz(win.v[slot]);
+        nframe.identity = wn.w != 0.0f;
+        float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(p.perturbations + b))));
+        float3 rd = qs::normalize(qs::reflect(neg(dir), n));
+        const float3 origin = xyz(win.o[slot]);
+        if (collide(G, T.own, origin, rd, flags)) {
+          code = kBlocked;
         } else {
-          float e = qs::ray_energy(tt, rd, n, factor);
-          int row = int(qm_rn_mul(uu, (float)R.resolution.y));
-          int col = int(qm_rn_mul(vv, (float)R.resolution.x));
-          if (row >= R.resolution.y || col >= R.resolution.x || row < 0 || col < 0) {
-            row = min(max(row, 0), R.resolution.y - 1);
-            col = min(max(col, 0), R.resolution.x - 1);
-            ++clamped;
+          float tt, uu, vv;
+          if (!receiver_hit(R, origin, rd, tt, uu, vv)) {
+            code = kMissed;
+          } else {
+            float e = qs::ray_energy(tt, rd, n, T.factor);
+            int row = int(qm_rn_mul(uu, (float)R.resolution.y));
+            int col = int(qm_rn_mul(vv, (float)R.resolution.x));
+            if (row >= R.resolution.y || col >= R.resolution.x || row < 0 || col < 0) {
+              row = min(max(row, 0), R.resolution.y - 1);
+              col = min(max(col, 0), R.resolution.x - 1);
+              ++clamped;
+            }
+            const int pix = row * R.resolution.x + col;
+            atomicAdd(R.image + pix, e);
+            power += (double)e;
+            code = pix;
           }
-          const int pix = row * R.resolution.x + col;
-          atomicAdd(R.image + pix, e);
-          power += (double)e;
-          code = pix;
         }
       }
+      if (kRecord) p.records[(size_t)(f - p.record_facet_begin) * nl + l] = code;
     }
-    if (kRecord) p.records[(size_t)(f - p.record_facet_begin) * nl + (l - p.light_begin)] = code;
+    f += q32;
+    l += r32;
+    if (l >= nl) {
+      l -= nl;
+      ++f;
+    }
   }
   for (int off = 16; off > 0; off >>= 1) {
     power += __shfl_down_sync(0xffffffffu, power, off);
@@ -394,9 +495,13 @@ cudaError_t QM_SYM(launch_facets)(const DevTask& task, float3* origins, float3* 
 
 int QM_SYM(trace_chunk_rays)() { return kChunk; }
 
-cudaError_t QM_SYM(launch_trace)(const TraceParams& p, bool record, cudaStream_t stream) {
-  const int threads = 256;
-  const long long nl = p.light_end - p.light_begin;
+cudaError_t QM_SYM(launch_trace)(const TraceParams& params, bool record, cudaStream_t stream) {
+  const int threads = kThreads;
+  const long long nl = params.light_end - params.light_begin;
+  if (nl <= 0) return cudaSuccess;
+  TraceParams p = params;
+  p.lights_q32 = (int)(32 / nl);
+  p.lights_r32 = (int)(32 % nl);
   const long long warps = record ? ((long long)(p.record_facet_end - p.record_facet_begin) * nl + kChunk - 1) / kChunk
                                  : p.total_facets;
   if (warps <= 0) return cudaSuccess;
