@@ -50,6 +50,15 @@ int qmcrt_scene_load(const char* scene_path, const char* config_path, int device
 /* Replaces SolarScene::clear (Scene/SolarScene.cpp:31-46). */
 void qmcrt_scene_free(qmcrt_scene* scene);
 
+/* New sun direction (direction of travel, as the configuration's "sun_dir").
+ * Replaces reloading the configuration and re-running the sun-dependent half
+ * of SceneProcessor::processScene (Scene/SceneProcessor.cpp:22-46:
+ * Heliostat::CSetNormalAndRotate per heliostat and Sunray::setSunDirection):
+ * heliostat normals, sub-heliostat parallelograms, traversal records and the
+ * world-space sun-shape pool are rebuilt; pools, facet offsets, images and
+ * powers are kept (clear them before tracing the new sun). */
+int qmcrt_scene_set_sun(qmcrt_scene* scene, const float* sun_dir3);
+
 typedef struct {
   int num_receivers, num_grids, num_heliostats;
   int num_sunshape_groups, num_per_sunshape_group, pool_size;
@@ -148,6 +157,45 @@ int qmcrt_diagnostics(qmcrt_scene* scene, unsigned long long* out4);
  * scratch; scene images and powers are untouched. */
 int qmcrt_debug_hit_records(qmcrt_scene* scene, int heliostat, int facet_begin, int facet_end,
                             int light_begin, int light_end, int* codes);
+
+/* ---- batched tracing ------------------------------------------------------
+ * No single reference counterpart: the reference traces one sun per
+ * processed scene, one heliostat per QuasiMonteCarloRayTracer::rayTracing
+ * call (QuasiMonteCarloRayTracer.cpp:15-91), looped by RayTracingPipeline
+ * (RayTracingPipeline.cpp:66-81).  A batch holds n instances, each a
+ * (scene, sun direction) pair with its own receiver images and FP64
+ * per-heliostat powers; the sun-dependent half of SceneProcessor::processScene
+ * (Scene/SceneProcessor.cpp:22-46) runs on the device for all instances, and
+ * qmcrt_batch_trace traces every heliostat of every instance in one launch.
+ * Instances share their scene's grid cell lists, sample pools and facet
+ * offsets (as read when the batch is created or its suns are set); scenes
+ * must outlive the batch and live on one device.  Light ranges are common to
+ * all instances (at most the smallest lights-per-group of the scenes). */
+typedef struct qmcrt_batch qmcrt_batch;
+int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scene_of_instance,
+                       const float* sun_dirs3, int n_instances, qmcrt_batch** out);
+void qmcrt_batch_free(qmcrt_batch* batch);
+/* New sun directions (3 floats per instance), prepared on the device. */
+int qmcrt_batch_set_suns(qmcrt_batch* batch, const float* sun_dirs3, void* stream);
+int qmcrt_batch_set_light_range(qmcrt_batch* batch, int begin, int end);
+int qmcrt_batch_set_math_mode(qmcrt_batch* batch, int mode);
+int qmcrt_batch_info(const qmcrt_batch* batch, int* instances, int* tasks, long long* rays_per_trace);
+int qmcrt_batch_trace(qmcrt_batch* batch, void* stream);
+/* Captures (optionally a clear of images and powers, then) one trace into a
+ * CUDA graph; qmcrt_batch_graph_launch replays it.  Changing the light range
+ * or math mode drops the graph. */
+int qmcrt_batch_capture_graph(qmcrt_batch* batch, int clear_first);
+int qmcrt_batch_graph_launch(qmcrt_batch* batch, void* stream);
+int qmcrt_batch_clear(qmcrt_batch* batch, void* stream);
+int qmcrt_batch_image(qmcrt_batch* batch, int instance, int receiver, float* out, int* width, int* height);
+int qmcrt_batch_power_fp64(qmcrt_batch* batch, int instance, double* per_heliostat, double* total);
+/* Times the production kernel builds (modes 0 and 2, identical results) on
+ * this batch and keeps the faster; images and powers are cleared after. */
+int qmcrt_batch_autotune(qmcrt_batch* batch, void* stream, int* chosen_mode, float* ms);
+/* Debug: the device-prepared sub-heliostat vertices (B, A, C per
+ * sub-heliostat, as qmcrt_grid_vertices) of one instance-grid and the
+ * heliostat normals of one instance (either output may be NULL). */
+int qmcrt_batch_debug_geometry(qmcrt_batch* batch, int instance, int grid, float* vertices, float* normals);
 
 /* ---- smoothing and output ------------------------------------------------
  * Replaces ImageSmoother::image_smooth (Tool/Smoother/ImageSmoother.cu:68-113):

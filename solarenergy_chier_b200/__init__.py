@@ -7,6 +7,7 @@ csrc/) does all the work; this package is its Python binding.
 from ._lib import LIB_PATH, QmcrtError, load  # noqa: F401
 from .scene import (  # noqa: F401
     SUNSHAPE_BUIE,
+    Batch,
     SUNSHAPE_PILLBOX,
     ImageSaver,
     ImageSmoother,
@@ -20,7 +21,7 @@ from .scene import (  # noqa: F401
 )
 
 __all__ = [
-    "Scene", "QuasiMonteCarloRayTracer", "ImageSmoother", "ImageSaver", "RayTracingPipeline",
+    "Scene", "Batch", "QuasiMonteCarloRayTracer", "ImageSmoother", "ImageSaver", "RayTracingPipeline",
     "SUNSHAPE_BUIE", "SUNSHAPE_PILLBOX", "QmcrtError", "load", "LIB_PATH", "save_text", "smooth_device",
     "pipeline_run", "executable",
 ]

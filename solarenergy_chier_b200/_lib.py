@@ -47,6 +47,7 @@ PROTOTYPES = {
     "qmcrt_version": (_i, []),
     "qmcrt_scene_load": (_i, [ctypes.c_char_p, ctypes.c_char_p, _i, _u, ctypes.POINTER(_vp)]),
     "qmcrt_scene_free": (None, [_vp]),
+    "qmcrt_scene_set_sun": (_i, [_vp, _pf]),
     "qmcrt_scene_get_info": (_i, [_vp, ctypes.POINTER(SceneInfo)]),
     "qmcrt_receiver_get": (_i, [_vp, _i, _pi, _pi, _pi, _pf, _pf, _pf, _pf]),
     "qmcrt_heliostat_get": (_i, [_vp, _i, _pi, _pi, _pi, _pi, _pi, _pf, _pf, _pf, _pf]),
@@ -76,6 +77,20 @@ PROTOTYPES = {
     "qmcrt_load_tasks": (_i, [_vp, ctypes.c_char_p, _pi, _pi, _i, _pi, _pi, _pi]),
     "qmcrt_save_text": (_i, [ctypes.c_char_p, _i, _i, _pf, _i, _pf]),
     "qmcrt_pipeline_run": (_i, [_i, ctypes.POINTER(ctypes.c_char_p)]),
+    "qmcrt_batch_create": (_i, [ctypes.POINTER(_vp), _i, _pi, _pf, _i, ctypes.POINTER(_vp)]),
+    "qmcrt_batch_free": (None, [_vp]),
+    "qmcrt_batch_set_suns": (_i, [_vp, _pf, _vp]),
+    "qmcrt_batch_set_light_range": (_i, [_vp, _i, _i]),
+    "qmcrt_batch_set_math_mode": (_i, [_vp, _i]),
+    "qmcrt_batch_info": (_i, [_vp, _pi, _pi, ctypes.POINTER(ctypes.c_longlong)]),
+    "qmcrt_batch_trace": (_i, [_vp, _vp]),
+    "qmcrt_batch_capture_graph": (_i, [_vp, _i]),
+    "qmcrt_batch_graph_launch": (_i, [_vp, _vp]),
+    "qmcrt_batch_clear": (_i, [_vp, _vp]),
+    "qmcrt_batch_image": (_i, [_vp, _i, _i, _pf, _pi, _pi]),
+    "qmcrt_batch_power_fp64": (_i, [_vp, _i, _pd, _pd]),
+    "qmcrt_batch_autotune": (_i, [_vp, _vp, _pi, _pf]),
+    "qmcrt_batch_debug_geometry": (_i, [_vp, _i, _i, _pf, _pf]),
 }
 
 _lib = None

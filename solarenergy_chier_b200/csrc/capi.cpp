@@ -1,10 +1,10 @@
 // C ABI (include/qmcrt.h) over the host scene model and the sm_100a kernels.
 #include "qmcrt.h"
+#include "helio_geom.h"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,306 +20,100 @@
 #include "smooth.h"
 #include "tracer.h"
 #include "vecmath.h"
+#include "runtime.h"
 
 namespace {
-
 thread_local std::string g_last_error;
-
-struct ApiError : std::runtime_error {
-  int code;
-  ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
-
-void cuda_check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw ApiError(QMCRT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <class F>
-int guarded(F&& f) {
-  try {
-    f();
-    g_last_error.clear();
-    return QMCRT_OK;
-  } catch (const ApiError& e) {
-    g_last_error = e.what();
-    return e.code;
-  } catch (const std::bad_alloc&) {
-    g_last_error = "host allocation failed";
-    return QMCRT_ERR_CUDA;
-  } catch (const std::exception& e) {
-    g_last_error = e.what();
-    return QMCRT_ERR_INVALID;
-  }
-}
-
-[[noreturn]] void invalid(const std::string& m) { throw ApiError(QMCRT_ERR_INVALID, m); }
-
-// Device buffer owned by the scene.
-struct DBuf {
-  void* p = nullptr;
-  size_t bytes = 0;
-  DBuf() = default;
-  DBuf(const DBuf&) = delete;
-  DBuf& operator=(const DBuf&) = delete;
-  ~DBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  void alloc(size_t n) {
-    if (n == bytes && p) return;
-    release();
-    if (n == 0) return;
-    cuda_check(cudaMalloc(&p, n), "cudaMalloc");
-    bytes = n;
-  }
-  template <class T>
-  T* as() const {
-    return static_cast<T*>(p);
-  }
-};
-
-template <class T>
-void upload(DBuf& b, const std::vector<T>& v) {
-  b.alloc(v.size() * sizeof(T));
-  if (!v.empty()) cuda_check(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
-}
-
-struct GridBufs {
-  DBuf hindex, hmatch, bound, hsub, subv;
-};
-
-class DeviceGuard {
- public:
-  explicit DeviceGuard(int dev) {
-    cudaGetDevice(&prev_);
-    if (prev_ != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
-    switched_ = prev_ != dev;
-  }
-  ~DeviceGuard() {
-    if (switched_) cudaSetDevice(prev_);
-  }
-
- private:
-  int prev_ = 0;
-  bool switched_ = false;
-};
-
 }  // namespace
 
 namespace qm {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace qm
 
-struct qmcrt_scene {
-  int device = 0;
-  unsigned seed = 0;
-  qm::SceneModel model;
-  std::vector<std::unique_ptr<GridBufs>> grid_bufs;
-  std::vector<qm::DevGrid> grids;
-  DBuf d_grids;
-  std::vector<std::unique_ptr<DBuf>> images;
-  std::vector<qm::DevReceiver> receivers;
-  DBuf d_receivers;
-  DBuf d_local;  // focus-flat local centres then normals
-  std::vector<long long> local_base;
-  DBuf d_offsets;
-  std::vector<long long> offset_base;
-  DBuf d_samples, d_perturb;
-  int pool_size = 0;
-  DBuf d_power, d_diag;
-  std::vector<qm::DevTask> templates;
-  DBuf d_tasks, d_prefix;
-  std::vector<int> cached_ids;
-  long long cached_lights = -1;
-  bool cache_valid = false;
-  qm::DevTask* h_stage = nullptr;  // pinned staging for task uploads
-  long long* h_prefix = nullptr;
-  size_t stage_cap = 0;
-  cudaEvent_t stage_done = nullptr;
-  qm::SunFrame sun{};
-  int exact = 0;
-  int light_begin = 0, light_end = 0;
-  long long total_facets = 0;
+using namespace qrt;
 
-  ~qmcrt_scene() {
-    if (device < 0) return;
-    int prev = 0;
-    cudaGetDevice(&prev);
-    cudaSetDevice(device);
-    cudaDeviceSynchronize();
-    if (h_stage) cudaFreeHost(h_stage);
-    if (h_prefix) cudaFreeHost(h_prefix);
-    if (stage_done) cudaEventDestroy(stage_done);
-    grid_bufs.clear();
-    images.clear();
-    d_grids.release();
-    d_receivers.release();
-    d_local.release();
-    d_offsets.release();
-    d_samples.release();
-    d_perturb.release();
-    d_power.release();
-    d_diag.release();
-    d_tasks.release();
-    d_prefix.release();
-    cudaSetDevice(prev);
-  }
-};
-
-namespace {
+namespace qrt {
 
 using qm::DevGrid;
 using qm::DevReceiver;
 using qm::DevTask;
 
-// Traversal record of one heliostat: a padded bounding box in a frame
-// aligned with its sub-heliostat lattice, and the lattice itself, so that a
-// ray entering the box only tests the sub-heliostats under its path.
-//
-// Frame: ex along the summed column edges (vertex A -> C of every
-// sub-heliostat), ez along the summed row edges (A -> B) made orthogonal to
-// ex, and their normal.  Box: the extent of every sub-heliostat corner along
-// the three axes, widened by `margin` (1 cm plus 1e-5 of the coordinate
-// scale, far above the float rounding of the box and parallelogram tests).
-//
-// Lattice: column c of the heliostat is assigned the band
-// [x0 + c px, x0 + (c+1) px] along ex, row r the band [z0 + r pz, z0 + (r+1) pz]
-// along ez (bands fitted to the column and row extents, gap-centred).  The
-// slack is the largest distance by which any corner of a sub-heliostat leaves
-// its band; the window margin is margin + slack.  A ray hitting sub-heliostat
-// (r, c) does so at a point whose ex coordinate lies in column c's band
-// widened by the window margin and inside the ray's own ex range within the
-// box, so the columns whose widened band meets that range (and likewise the
-// rows) hold every sub-heliostat the ray can hit, whatever the geometry: an
-// irregular layout only widens the window.  Degenerate frames fall back to a
-// window covering every sub-heliostat.
-//
-// Output (5 float4): centre.xyz + window margin; (ex, half_x); (n, half_n);
-// (ez, half_z); (x0, 1/px, z0, 1/pz).  rows_cols receives the lattice shape
-// (rows * cols == num_sub).
-void heliostat_box(const qm::HeliostatModel& h, const std::vector<float3>& verts, float4 out[5], int2& rows_cols) {
-  using D3 = std::array<double, 3>;
-  auto dot = [](const D3& a, const D3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
-  auto unit = [&](D3& a) {
-    double l = std::sqrt(dot(a, a));
-    if (!(l > 0) || !std::isfinite(l)) return false;
-    for (double& x : a) x /= l;
-    return true;
-  };
-  auto cross = [](const D3& a, const D3& b) {
-    return D3{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
-  };
-  const int ns = h.num_sub;
-  int rows = h.row_col.x, cols = h.row_col.y;
-  bool lattice = ns > 1 && rows > 0 && cols > 0 && rows * cols == ns;
-  if (!lattice) {
-    rows = 1;
-    cols = std::max(ns, 1);
+// Sun-dependent data of one grid: per heliostat its traversal record and
+// (first sub-heliostat, count, lattice rows, lattice columns), and per
+// sub-heliostat its parallelogram as A, B - A, C - A.
+void grid_sun_data(const qm::SceneModel& m, const qm::GridModel& g, std::vector<float4>& bound,
+                   std::vector<int4>& hsub, std::vector<float4>& subv) {
+  bound.assign(5 * (size_t)g.num_heliostats, float4{});
+  hsub.assign(g.num_heliostats, int4{});
+  for (int i = 0; i < g.num_heliostats; ++i) {
+    const qm::HeliostatModel& h = m.heliostats[g.start_heliostat + i];
+    int2 rc;
+    qm::heliostat_record(g.sub_vertices.data() + 3 * (size_t)h.sub_begin, h.num_sub, h.row_col, h.pos, h.normal,
+                         &bound[5 * (size_t)i], &rc);
+    hsub[i] = make_int4(h.sub_begin, h.num_sub, rc.x, rc.y);
   }
-  std::vector<std::array<D3, 4>> corners(ns);
-  D3 sx{0, 0, 0}, sz{0, 0, 0};
-  for (int k = 0; k < ns; ++k) {
-    const int s = h.sub_begin + k;
-    const float3 B = verts[3 * s], A = verts[3 * s + 1], C = verts[3 * s + 2];
-    const D3 a{A.x, A.y, A.z};
-    const D3 ab{(double)B.x - A.x, (double)B.y - A.y, (double)B.z - A.z};
-    const D3 ac{(double)C.x - A.x, (double)C.y - A.y, (double)C.z - A.z};
-    for (int corner = 0; corner < 4; ++corner)
-      for (int i = 0; i < 3; ++i)
-        corners[k][corner][i] = a[i] + ((corner & 1) ? ab[i] : 0.0) + ((corner & 2) ? ac[i] : 0.0);
-    for (int i = 0; i < 3; ++i) {
-      sx[i] += ac[i];
-      sz[i] += ab[i];
+  subv.assign(3 * (size_t)g.num_subheliostats, float4{});
+  for (int sidx = 0; sidx < g.num_subheliostats; ++sidx) {
+    const float3 B = g.sub_vertices[3 * sidx], A = g.sub_vertices[3 * sidx + 1], C = g.sub_vertices[3 * sidx + 2];
+    const float3 ab = qm::sub(B, A), ac = qm::sub(C, A);
+    subv[3 * sidx] = make_float4(A.x, A.y, A.z, ab.x);
+    subv[3 * sidx + 1] = make_float4(ab.y, ab.z, ac.x, ac.y);
+    subv[3 * sidx + 2] = make_float4(ac.z, 0.f, 0.f, 0.f);
+  }
+}
+
+// Sun frame and per-heliostat task templates (both depend on the sun).
+void build_templates(qmcrt_scene* s) {
+  const qm::SceneModel& m = s->model;
+  const qm::SceneConfig& cfg = m.config;
+  // Sun frame of -sun_dir (QuasiMonteCarloRayTracer::generateSunrayArgument feeds
+  // -sunray_direction to local2world_rotate per ray; the frame is constant).
+  qm::Frame f = qm::make_frame(qm::neg(cfg.sun_dir), false);
+  s->sun.u = f.u;
+  s->sun.n = f.n;
+  s->sun.v = f.v;
+  s->sun.identity = f.identity ? 1 : 0;
+
+  s->templates.assign(m.heliostats.size(), DevTask{});
+  for (size_t i = 0; i < m.heliostats.size(); ++i) {
+    const auto& h = m.heliostats[i];
+    const auto& g = m.grids[h.grid];
+    const auto& r = m.receivers[g.receiver];
+    DevTask t{};
+    t.type = h.type;
+    t.grid = h.grid;
+    t.receiver = g.receiver;
+    t.own = (int)i - g.start_heliostat;
+    t.num_facets = h.num_facets;
+    t.power_slot = (int)i;
+    t.row_col = h.row_col;
+    t.sub_row_col = h.sub_row_col;
+    t.pixel_length = h.pixel_length;
+    // QuasiMonteCarloRayTracer::rayTracing (QuasiMonteCarloRayTracer.cpp:58-60).
+    float ratio = h.pixel_length / r.pixel_length;
+    t.factor = cfg.dni * ratio * ratio * cfg.helio_reflected_rate / float(cfg.num_per_sunshape_group);
+    t.gap = h.gap;
+    t.sub_length = h.sub_length;
+    t.size = h.size;
+    t.pos = h.pos;
+    t.normal = h.normal;
+    qm::Frame hf = qm::make_frame(h.normal, h.type == 1);
+    t.fu = hf.u;
+    t.fn = hf.n;
+    t.fv = hf.v;
+    t.frame_identity = hf.identity ? 1 : 0;
+    if (h.type == 1) {
+      const float3* base = s->d_local.as<float3>() + s->local_base[i];
+      t.local_centers = base;
+      t.local_normals = base + h.local_centers.size();
     }
+    t.offsets = s->d_offsets.as<int>() + s->offset_base[i];
+    t.samples = s->d_trace_samples.as<float4>();
+    t.perturbations = s->d_trace_perturb.as<float4>();
+    t.pool_size = s->pool_size;
+    s->templates[i] = t;
   }
-  D3 ex = sx, ez = sz, n{0, 0, 0};
-  bool frame = unit(ex);
-  if (frame) {
-    const double p = dot(ez, ex);
-    for (int i = 0; i < 3; ++i) ez[i] -= p * ex[i];
-    frame = unit(ez);
-  }
-  if (frame) {
-    n = cross(ez, ex);
-    frame = unit(n);
-  }
-  if (!frame) {
-    // Any orthonormal frame around the heliostat normal; no lattice.
-    n = D3{h.normal.x, h.normal.y, h.normal.z};
-    if (!unit(n)) n = D3{0, 1, 0};
-    ex = std::fabs(n[0]) < 0.9 ? D3{0, -n[2], n[1]} : D3{-n[1], n[0], 0};
-    unit(ex);
-    ez = cross(ex, n);
-    lattice = false;
-    rows = 1;
-    cols = std::max(ns, 1);
-  }
-  const D3* ax[3] = {&ex, &n, &ez};
-  const D3 c0{h.pos.x, h.pos.y, h.pos.z};
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  double maxabs = std::fabs(c0[0]) + std::fabs(c0[1]) + std::fabs(c0[2]);
-  for (int k = 0; k < ns; ++k)
-    for (const D3& q : corners[k]) {
-      const D3 p{q[0] - c0[0], q[1] - c0[1], q[2] - c0[2]};
-      for (int a = 0; a < 3; ++a) {
-        const double d = dot(p, *ax[a]);
-        lo[a] = std::min(lo[a], d);
-        hi[a] = std::max(hi[a], d);
-      }
-      maxabs = std::max(maxabs, std::fabs(q[0]) + std::fabs(q[1]) + std::fabs(q[2]));
-    }
-  const double margin = 0.01 + 1e-5 * maxabs;
-  D3 centre = c0;
-  double half[3];
-  for (int a = 0; a < 3; ++a) {
-    const double mid = 0.5 * (lo[a] + hi[a]);
-    for (int i = 0; i < 3; ++i) centre[i] += mid * (*ax[a])[i];
-    half[a] = 0.5 * (hi[a] - lo[a]) + margin;
-  }
-  // Lattice bands in box-centre coordinates.
-  double x0 = 0, px = 1, z0 = 0, pz = 1, slack = 0;
-  if (lattice) {
-    std::vector<double> xl(cols, 1e300), xh(cols, -1e300), zl(rows, 1e300), zh(rows, -1e300);
-    for (int k = 0; k < ns; ++k) {
-      const int r = k / cols, c = k % cols;
-      for (const D3& q : corners[k]) {
-        const D3 p{q[0] - centre[0], q[1] - centre[1], q[2] - centre[2]};
-        const double x = dot(p, ex), z = dot(p, ez);
-        xl[c] = std::min(xl[c], x);
-        xh[c] = std::max(xh[c], x);
-        zl[r] = std::min(zl[r], z);
-        zh[r] = std::max(zh[r], z);
-      }
-    }
-    auto fit = [&](const std::vector<double>& l, const std::vector<double>& u, double& b0, double& pitch) {
-      const int m = (int)l.size();
-      double gap = 0;
-      for (int i = 0; i + 1 < m; ++i) gap += l[i + 1] - u[i];
-      gap = m > 1 ? gap / (m - 1) : 0.0;
-      pitch = (u[m - 1] - l[0] + gap) / m;
-      b0 = l[0] - 0.5 * gap;
-      if (!(pitch > 0) || !std::isfinite(pitch)) return false;
-      for (int i = 0; i < m; ++i) {
-        slack = std::max(slack, (b0 + i * pitch) - l[i]);
-        slack = std::max(slack, u[i] - (b0 + (i + 1) * pitch));
-      }
-      return true;
-    };
-    lattice = fit(xl, xh, x0, px) && fit(zl, zh, z0, pz) && std::isfinite(slack);
-  }
-  const double window = lattice ? margin + slack : 1e30;
-  if (!lattice) {
-    x0 = z0 = 0;
-    px = pz = 1;
-  }
-  out[0] = make_float4((float)centre[0], (float)centre[1], (float)centre[2], (float)window);
-  for (int a = 0; a < 3; ++a)
-    out[1 + a] = make_float4((float)(*ax[a])[0], (float)(*ax[a])[1], (float)(*ax[a])[2], (float)(half[a] * (1 + 1e-6)));
-  // A single column (row) maps every x (z) to band 0.
-  out[4] = make_float4((float)x0, cols > 1 ? (float)(1.0 / px) : 0.0f, (float)z0, rows > 1 ? (float)(1.0 / pz) : 0.0f);
-  rows_cols = make_int2(rows, cols);
+  s->cache_valid = false;
 }
 
 void build_device_scene(qmcrt_scene* s) {
@@ -339,24 +133,11 @@ void build_device_scene(qmcrt_scene* s) {
     auto gb = std::make_unique<GridBufs>();
     upload(gb->hindex, g.cell_hindex);
     upload(gb->hmatch, g.cell_hmatch);
-    std::vector<float4> bound(5 * (size_t)g.num_heliostats);
-    std::vector<int4> hsub(g.num_heliostats);
-    for (int i = 0; i < g.num_heliostats; ++i) {
-      const qm::HeliostatModel& h = m.heliostats[g.start_heliostat + i];
-      int2 rc;
-      heliostat_box(h, g.sub_vertices, &bound[5 * (size_t)i], rc);
-      hsub[i] = make_int4(h.sub_begin, h.num_sub, rc.x, rc.y);
-    }
+    std::vector<float4> bound, subv;
+    std::vector<int4> hsub;
+    grid_sun_data(m, g, bound, hsub, subv);
     upload(gb->bound, bound);
     upload(gb->hsub, hsub);
-    std::vector<float4> subv(3 * (size_t)g.num_subheliostats);
-    for (int sidx = 0; sidx < g.num_subheliostats; ++sidx) {
-      const float3 B = g.sub_vertices[3 * sidx], A = g.sub_vertices[3 * sidx + 1], C = g.sub_vertices[3 * sidx + 2];
-      const float3 ab = qm::sub(B, A), ac = qm::sub(C, A);
-      subv[3 * sidx] = make_float4(A.x, A.y, A.z, ab.x);
-      subv[3 * sidx + 1] = make_float4(ab.y, ab.z, ac.x, ac.y);
-      subv[3 * sidx + 2] = make_float4(ac.z, 0.f, 0.f, 0.f);
-    }
     upload(gb->subv, subv);
     DevGrid dg;
     dg.pos = g.pos;
@@ -422,66 +203,38 @@ void build_device_scene(qmcrt_scene* s) {
 
   s->d_samples.alloc((size_t)P * sizeof(float4));
   s->d_perturb.alloc((size_t)P * sizeof(float4));
+  s->d_trace_samples.alloc((size_t)(P + cfg.num_per_sunshape_group) * sizeof(float4));
+  s->d_trace_perturb.alloc((size_t)(P + cfg.num_per_sunshape_group) * sizeof(float4));
+  {
+    std::vector<long long> seg(s->offset_base);
+    seg.push_back(total);
+    upload(s->d_offset_seg, seg);
+  }
   s->d_power.alloc(std::max<size_t>(m.heliostats.size(), 1) * sizeof(double));
   cuda_check(cudaMemset(s->d_power.p, 0, s->d_power.bytes), "cudaMemset");
   s->d_diag.alloc(qm::kDiagSlots * sizeof(unsigned long long));
   cuda_check(cudaMemset(s->d_diag.p, 0, s->d_diag.bytes), "cudaMemset");
 
-  // Sun frame of -sun_dir (QuasiMonteCarloRayTracer::generateSunrayArgument feeds
-  // -sunray_direction to local2world_rotate per ray; the frame is constant).
-  qm::Frame f = qm::make_frame(qm::neg(cfg.sun_dir), false);
-  s->sun.u = f.u;
-  s->sun.n = f.n;
-  s->sun.v = f.v;
-  s->sun.identity = f.identity ? 1 : 0;
-
-  // Per-heliostat task templates.
-  s->templates.assign(m.heliostats.size(), DevTask{});
-  for (size_t i = 0; i < m.heliostats.size(); ++i) {
-    const auto& h = m.heliostats[i];
-    const auto& g = m.grids[h.grid];
-    const auto& r = m.receivers[g.receiver];
-    DevTask t{};
-    t.type = h.type;
-    t.grid = h.grid;
-    t.receiver = g.receiver;
-    t.own = (int)i - g.start_heliostat;
-    t.num_facets = h.num_facets;
-    t.power_slot = (int)i;
-    t.row_col = h.row_col;
-    t.sub_row_col = h.sub_row_col;
-    t.pixel_length = h.pixel_length;
-    // QuasiMonteCarloRayTracer::rayTracing (QuasiMonteCarloRayTracer.cpp:58-60).
-    float ratio = h.pixel_length / r.pixel_length;
-    t.factor = cfg.dni * ratio * ratio * cfg.helio_reflected_rate / float(cfg.num_per_sunshape_group);
-    t.gap = h.gap;
-    t.sub_length = h.sub_length;
-    t.size = h.size;
-    t.pos = h.pos;
-    t.normal = h.normal;
-    qm::Frame hf = qm::make_frame(h.normal, h.type == 1);
-    t.fu = hf.u;
-    t.fn = hf.n;
-    t.fv = hf.v;
-    t.frame_identity = hf.identity ? 1 : 0;
-    if (h.type == 1) {
-      const float3* base = s->d_local.as<float3>() + s->local_base[i];
-      t.local_centers = base;
-      t.local_normals = base + h.local_centers.size();
-    }
-    t.offsets = s->d_offsets.as<int>() + s->offset_base[i];
-    s->templates[i] = t;
-  }
+  build_templates(s);
   s->cache_valid = false;
 }
 
 void generate_offsets(qmcrt_scene* s, unsigned seed) {
-  for (size_t i = 0; i < s->model.heliostats.size(); ++i) {
-    long long n = (long long)s->model.heliostats[i].num_facets + 1;
-    cuda_check(qm::launch_offsets(s->d_offsets.as<int>() + s->offset_base[i], n, seed, (int)i, s->pool_size, 0),
-               "offsets kernel");
-  }
+  const long long total = (long long)(s->d_offsets.bytes / sizeof(int));
+  cuda_check(qm::launch_offsets_all(s->d_offsets.as<int>(), s->d_offset_seg.as<long long>(),
+                                    (int)s->model.heliostats.size(), total, seed, s->pool_size, 0),
+             "offsets kernel");
   cuda_check(cudaDeviceSynchronize(), "offsets kernel");
+}
+
+// The tracer's copies of the pools (world-space samples, P + L entries);
+// redone after every change of the pools or of the sun.
+void rotate_pool(qmcrt_scene* s) {
+  const int n_out = s->pool_size + s->model.config.num_per_sunshape_group;
+  cuda_check(qm::launch_trace_pools(s->d_samples.as<float4>(), s->d_perturb.as<float4>(), s->pool_size, n_out, s->sun,
+                                    s->d_trace_samples.as<float4>(), s->d_trace_perturb.as<float4>(), 0),
+             "pool rotation");
+  cuda_check(cudaDeviceSynchronize(), "pool rotation");
 }
 
 void generate_pool(qmcrt_scene* s, unsigned seed, int sunshape, float half_angle) {
@@ -514,6 +267,7 @@ void generate_pool(qmcrt_scene* s, unsigned seed, int sunshape, float half_angle
   }
   cuda_check(qm::launch_pool(p, 0), "pool kernel");
   cuda_check(cudaDeviceSynchronize(), "pool kernel");
+  rotate_pool(s);
 }
 
 qmcrt_scene* checked(qmcrt_scene* s) {
@@ -550,28 +304,20 @@ qm::TraceParams base_params(qmcrt_scene* s) {
   qm::TraceParams p{};
   p.grids = s->d_grids.as<DevGrid>();
   p.receivers = s->d_receivers.as<DevReceiver>();
-  p.samples = s->d_samples.as<float4>();
-  p.perturbations = s->d_perturb.as<float4>();
-  p.pool_size = s->pool_size;
   p.light_begin = s->light_begin;
   p.light_end = s->light_end;
-  p.sun = s->sun;
   p.power = s->d_power.as<double>();
   p.diag = s->d_diag.as<unsigned long long>();
   return p;
 }
 
-cudaError_t run_trace(qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st) {
+cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st) {
   switch (s->exact) {
     case 1: return qm::launch_trace_exact(p, record, st);
     case 2: return qm::launch_trace_fast4(p, record, st);
     default: return qm::launch_trace_fast(p, record, st);
   }
 }
-
-// Rays of one heliostat in one launch: the kernel indexes them with int,
-// with 2^16 of headroom for a warp's chunk past the end.
-constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;
 
 void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
   if (n < 0 || (n > 0 && !ids)) invalid("heliostat list is invalid");
@@ -614,7 +360,9 @@ void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
   cuda_check(run_trace(s, p, false, stream), "trace kernel");
 }
 
-}  // namespace
+int trace_chunk_rays() { return qm::trace_chunk_rays_fast(); }
+
+}  // namespace qrt
 
 extern "C" {
 
@@ -794,6 +542,34 @@ int qmcrt_heliostat_facets(qmcrt_scene* s, int id, float* origins, float* normal
   });
 }
 
+int qmcrt_scene_set_sun(qmcrt_scene* s, const float* sun_dir) {
+  return guarded([&] {
+    if (!s) invalid("scene is NULL");
+    if (!sun_dir) invalid("sun direction is NULL");
+    const float3 d = make_float3(sun_dir[0], sun_dir[1], sun_dir[2]);
+    if (!std::isfinite(d.x) || !std::isfinite(d.y) || !std::isfinite(d.z) || (d.x == 0 && d.y == 0 && d.z == 0))
+      invalid("sun direction must be finite and non-zero");
+    qm::set_sun(s->model, d);
+    if (s->device < 0) return;
+    DeviceGuard guard(s->device);
+    cuda_check(cudaDeviceSynchronize(), "set_sun");
+    for (size_t g = 0; g < s->model.grids.size(); ++g) {
+      std::vector<float4> bound, subv;
+      std::vector<int4> hsub;
+      grid_sun_data(s->model, s->model.grids[g], bound, hsub, subv);
+      upload(s->grid_bufs[g]->bound, bound);
+      upload(s->grid_bufs[g]->hsub, hsub);
+      upload(s->grid_bufs[g]->subv, subv);
+      s->grids[g].bound = s->grid_bufs[g]->bound.as<float4>();
+      s->grids[g].hsub = s->grid_bufs[g]->hsub.as<int4>();
+      s->grids[g].subv = s->grid_bufs[g]->subv.as<float4>();
+    }
+    upload(s->d_grids, s->grids);
+    build_templates(s);
+    rotate_pool(s);
+  });
+}
+
 int qmcrt_set_sample_pool(qmcrt_scene* s, const float* dirs, const float* perturb, int groups, int per_group,
                           int on_device) {
   return guarded([&] {
@@ -812,6 +588,7 @@ int qmcrt_set_sample_pool(qmcrt_scene* s, const float* dirs, const float* pertur
     cuda_check(cudaMemcpy(tmp.p, perturb, (size_t)n * 3 * sizeof(float), kind), "pool upload");
     cuda_check(qm::launch_xyz_to_float4(tmp.as<float>(), s->d_perturb.as<float4>(), n, 0), "pool convert");
     cuda_check(cudaDeviceSynchronize(), "pool convert");
+    rotate_pool(s);
   });
 }
 

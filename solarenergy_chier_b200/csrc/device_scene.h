@@ -53,6 +53,9 @@ struct DevTask {
   const float3* local_centers;  // focus-flat: per sub-heliostat
   const float3* local_normals;
   const int* offsets;   // num_facets + 1 pool offsets
+  const float4* samples;        // sun-shape pool already turned into world space by this task's sun
+  const float4* perturbations;  // slope-error pool (local frame of the facet normal)
+  int pool_size;                // P = groups x lights per group
 };
 
 struct SunFrame {
@@ -74,12 +77,8 @@ struct TraceParams {
   const long long* facet_prefix;  // num_tasks + 1 prefix sums of warp chunks per task
   int num_tasks;
   long long total_facets;         // total warp chunks of the launch
-  const float4* samples;          // sun-shape pool, P entries (xyz used)
-  const float4* perturbations;    // slope-error pool, P entries
-  int pool_size;
   int light_begin, light_end;     // light indexes traced per facet
   int lights_q32, lights_r32;     // 32 / (light_end - light_begin) and 32 % it (set by the launcher)
-  SunFrame sun;                   // frame of -sun_dir
   double* power;                  // FP64 per-slot power accumulators
   unsigned long long* diag;
   // hit-record variant only

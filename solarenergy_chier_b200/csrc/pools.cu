@@ -6,6 +6,7 @@
 // a pool exactly; the mapping from uniforms to directions follows the
 // reference.
 #include "pools.h"
+#include "device_scene.h"
 #include "sampling.h"
 #include "vecmath.h"
 
@@ -82,6 +83,42 @@ __global__ void offsets_kernel(int* out, long long count, uint32_t seed, int hel
   out[i] = facet_offset(seed, (uint32_t)heliostat, (uint32_t)i, (uint32_t)pool);
 }
 
+// Facet offsets of every heliostat in one launch: element i of the buffer
+// belongs to heliostat h with seg[h] <= i < seg[h + 1].
+__global__ void offsets_all_kernel(int* out, const long long* seg, int heliostats, uint32_t seed, int pool) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= seg[heliostats]) return;
+  int lo = 0, hi = heliostats - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg[mid] <= i) lo = mid; else hi = mid - 1;
+  }
+  out[i] = facet_offset(seed, (uint32_t)lo, (uint32_t)(i - seg[lo]), (uint32_t)pool);
+}
+
+// The pools as the tracer reads them: n_out = P + L entries, entry i holding
+// pool entry i % P, so that offset + light index never wraps; sun-shape
+// samples turned into world space by the sun frame, exactly as the reference
+// turns each one per ray (local2world_rotate of the sample about
+// -sun_direction, RectangleReceiverRectangleGridRayTracing.cu:16).
+__global__ void trace_pools_kernel(const float4* in, const float4* pert, int n, int n_out, SunFrame sun, float4* out,
+                                   float4* pert_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_out) return;
+  const int k = i % n;
+  pert_out[i] = pert[k];
+  float3 d = make_float3(in[k].x, in[k].y, in[k].z);
+  if (!sun.identity) {
+    Frame f;
+    f.u = sun.u;
+    f.n = sun.n;
+    f.v = sun.v;
+    f.identity = false;
+    d = qs::to_world(f, d);
+  }
+  out[i] = make_float4(d.x, d.y, d.z, 0.0f);
+}
+
 __global__ void xyz_to_float4_kernel(const float* xyz, float4* out, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -99,6 +136,20 @@ cudaError_t launch_pool(const PoolParams& p, cudaStream_t stream) {
 cudaError_t launch_offsets(int* out, long long count, uint32_t seed, int heliostat, int pool, cudaStream_t stream) {
   if (count <= 0) return cudaSuccess;
   offsets_kernel<<<(unsigned)((count + 255) / 256), 256, 0, stream>>>(out, count, seed, heliostat, pool);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_offsets_all(int* out, const long long* seg, int heliostats, long long total, uint32_t seed, int pool,
+                               cudaStream_t stream) {
+  if (total <= 0 || heliostats <= 0) return cudaSuccess;
+  offsets_all_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(out, seg, heliostats, seed, pool);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trace_pools(const float4* samples, const float4* perturbations, int n, int n_out,
+                               const SunFrame& sun, float4* out, float4* pert_out, cudaStream_t stream) {
+  if (n <= 0 || n_out <= 0) return cudaSuccess;
+  trace_pools_kernel<<<(n_out + 255) / 256, 256, 0, stream>>>(samples, perturbations, n, n_out, sun, out, pert_out);
   return cudaGetLastError();
 }
 

@@ -45,5 +45,13 @@ struct PoolParams {
 cudaError_t launch_pool(const PoolParams& p, cudaStream_t stream);
 cudaError_t launch_offsets(int* out, long long count, uint32_t seed, int heliostat, int pool, cudaStream_t stream);
 cudaError_t launch_xyz_to_float4(const float* xyz, float4* out, int n, cudaStream_t stream);
+// Offsets of all heliostats; seg (device) holds heliostats + 1 segment starts.
+cudaError_t launch_offsets_all(int* out, const long long* seg, int heliostats, long long total, uint32_t seed, int pool,
+                               cudaStream_t stream);
+struct SunFrame;
+// Tracer copies of the pools (n_out = P + L entries, entry i = pool entry
+// i % P; samples turned into world space by the sun frame).
+cudaError_t launch_trace_pools(const float4* samples, const float4* perturbations, int n, int n_out,
+                               const SunFrame& sun, float4* out, float4* pert_out, cudaStream_t stream);
 
 }  // namespace qm

@@ -1,0 +1,89 @@
+// Per-sun scene preparation on the device: for every (sun, heliostat) of a
+// batch, the sun-dependent half of SceneProcessor::processScene
+// (Scene/SceneProcessor.cpp:22-39): the heliostat normal
+// (Heliostat::CSetNormal, Heliostat.cu:15-20), its corner / sub-heliostat
+// parallelograms (Heliostat::CSetWorldVertex, Heliostat.cu:22-40;
+// FocusFlatRectangleHelio::CGetSubHeliostatVertexes, FocusFlatRectangleHelio.cu:123-227),
+// the traversal record and the tracer's facet frame; and the world-space
+// sun-shape pool of every sun.
+//
+// The arithmetic is helio_geom.h's, shared with the host scene code; this
+// unit is compiled with -fmad=false, so a heliostat prepared here equals the
+// host's bit for bit.
+#include "prep.h"
+
+#include "helio_geom.h"
+
+namespace qm {
+namespace {
+
+__global__ void prep_kernel(const PrepItem* items, int n, DevTask* tasks) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const PrepItem it = items[i];
+  DevTask& T = tasks[it.task];
+  const float3 normal = helio_normal(T.pos, it.focus, it.sun_dir);
+  T.normal = normal;
+  const Frame hf = qs::make_frame(normal, T.type == 1);
+  T.fu = hf.u;
+  T.fn = hf.n;
+  T.fv = hf.v;
+  T.frame_identity = hf.identity ? 1 : 0;
+  float3* v = it.verts;
+  if (T.type == 0) {
+    float3 c[4];
+    flat_vertices(T.size, normal, T.pos, c);
+    v[0] = c[0];
+    v[1] = c[1];
+    v[2] = c[2];
+  } else {
+    const float2 len = sub_lengths(T.size, T.gap, T.row_col);
+    for (int s = 0; s < it.num_sub; ++s)
+      focus_flat_sub_vertices(len, T.local_centers[s], T.local_normals[s], normal, T.pos, v + 3 * s);
+  }
+  for (int s = 0; s < it.num_sub; ++s) {
+    const float3 B = v[3 * s], A = v[3 * s + 1], C = v[3 * s + 2];
+    const float3 ab = qs::sub(B, A), ac = qs::sub(C, A);
+    it.subv[3 * s] = make_float4(A.x, A.y, A.z, ab.x);
+    it.subv[3 * s + 1] = make_float4(ab.y, ab.z, ac.x, ac.y);
+    it.subv[3 * s + 2] = make_float4(ac.z, 0.f, 0.f, 0.f);
+  }
+  int2 rc;
+  heliostat_record(v, it.num_sub, T.row_col, T.pos, normal, it.bound, &rc);
+  *it.hsub = make_int4(it.sub_first, it.num_sub, rc.x, rc.y);
+}
+
+// Pool of instance blockIdx.y turned by that instance's sun frame.
+__global__ void rotate_pools_kernel(const PoolRotation* jobs) {
+  const PoolRotation J = jobs[blockIdx.y];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= J.n_out) return;
+  const int k = i % J.n;
+  float3 d = make_float3(J.in[k].x, J.in[k].y, J.in[k].z);
+  if (!J.sun.identity) {
+    Frame f;
+    f.u = J.sun.u;
+    f.n = J.sun.n;
+    f.v = J.sun.v;
+    f.identity = false;
+    d = qs::to_world(f, d);
+  }
+  J.out[i] = make_float4(d.x, d.y, d.z, 0.0f);
+}
+
+}  // namespace
+
+cudaError_t launch_prep(const PrepItem* items, int n, DevTask* tasks, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  prep_kernel<<<(n + 127) / 128, 128, 0, stream>>>(items, n, tasks);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rotate_pools(const PoolRotation* jobs, int n_jobs, int max_out, cudaStream_t stream) {
+  if (n_jobs <= 0 || max_out <= 0) return cudaSuccess;
+  if (n_jobs > 65535) return cudaErrorInvalidValue;
+  rotate_pools_kernel<<<dim3((max_out + 255) / 256, n_jobs), 256, 0, stream>>>(jobs);
+  return cudaGetLastError();
+}
+
+}  // namespace qm

@@ -1,0 +1,37 @@
+// Device-side per-sun preparation (prep.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "device_scene.h"
+
+namespace qm {
+
+// One (sun, heliostat) to prepare.  The task already holds the heliostat's
+// sun-independent fields; the kernel fills its normal and facet frame and
+// writes the heliostat's sub-heliostat parallelograms and traversal record
+// into the sun's grid arrays.
+struct PrepItem {
+  int task;         // index into the task array
+  int num_sub;      // sub-heliostats of the heliostat
+  int sub_first;    // grid-local id of its first sub-heliostat
+  float3 focus;     // aim point (sun-independent)
+  float3 sun_dir;   // direction of travel of the sun's rays
+  float3* verts;    // out: 3 float3 (B, A, C) per sub-heliostat
+  float4* subv;     // out: 3 float4 per sub-heliostat (A, B - A, C - A)
+  float4* bound;    // out: 5 float4 traversal record
+  int4* hsub;       // out: (first, count, lattice rows, lattice columns)
+};
+
+struct PoolRotation {
+  const float4* in;  // local sun-shape pool, n entries
+  float4* out;       // world-space tracer copy, n_out = n + L entries (entry i = pool entry i % n)
+  int n, n_out;
+  SunFrame sun;
+};
+
+cudaError_t launch_prep(const PrepItem* items, int n, DevTask* tasks, cudaStream_t stream);
+// max_out: the largest n_out of the jobs.
+cudaError_t launch_rotate_pools(const PoolRotation* jobs, int n_jobs, int max_out, cudaStream_t stream);
+
+}  // namespace qm

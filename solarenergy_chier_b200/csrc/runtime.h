@@ -1,0 +1,181 @@
+// Internal runtime shared by the C ABI units (capi.cpp, batch.cpp): error
+// handling, device buffers and the scene state behind qmcrt_scene.  Not part
+// of the public interface (include/qmcrt.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "device_scene.h"
+#include "qmcrt.h"
+#include "scene.h"
+
+namespace qm {
+void set_last_error(const std::string& msg);
+}  // namespace qm
+
+namespace qrt {
+
+struct ApiError : std::runtime_error {
+  int code;
+  ApiError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+inline void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw ApiError(QMCRT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Runs one C ABI call: exceptions become status codes, their message the
+// thread's last error.
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    qm::set_last_error("");
+    return QMCRT_OK;
+  } catch (const ApiError& e) {
+    qm::set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    qm::set_last_error("host allocation failed");
+    return QMCRT_ERR_CUDA;
+  } catch (const std::exception& e) {
+    qm::set_last_error(e.what());
+    return QMCRT_ERR_INVALID;
+  }
+}
+
+[[noreturn]] inline void invalid(const std::string& m) { throw ApiError(QMCRT_ERR_INVALID, m); }
+
+// Device buffer owned by the scene.
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t n) {
+    if (n == bytes && p) return;
+    release();
+    if (n == 0) return;
+    cuda_check(cudaMalloc(&p, n), "cudaMalloc");
+    bytes = n;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+template <class T>
+void upload(DBuf& b, const std::vector<T>& v) {
+  b.alloc(v.size() * sizeof(T));
+  if (!v.empty()) cuda_check(cudaMemcpy(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+}
+
+struct GridBufs {
+  DBuf hindex, hmatch, bound, hsub, subv;
+};
+
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev_);
+    if (prev_ != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+    switched_ = prev_ != dev;
+  }
+  ~DeviceGuard() {
+    if (switched_) cudaSetDevice(prev_);
+  }
+
+ private:
+  int prev_ = 0;
+  bool switched_ = false;
+};
+
+}  // namespace qrt
+
+struct qmcrt_scene {
+  int device = 0;
+  unsigned seed = 0;
+  qm::SceneModel model;
+  std::vector<std::unique_ptr<qrt::GridBufs>> grid_bufs;
+  std::vector<qm::DevGrid> grids;
+  qrt::DBuf d_grids;
+  std::vector<std::unique_ptr<qrt::DBuf>> images;
+  std::vector<qm::DevReceiver> receivers;
+  qrt::DBuf d_receivers;
+  qrt::DBuf d_local;  // focus-flat local centres then normals
+  std::vector<long long> local_base;
+  qrt::DBuf d_offsets;
+  std::vector<long long> offset_base;
+  qrt::DBuf d_samples, d_perturb;
+  qrt::DBuf d_trace_samples;  // tracer copy: d_samples in world space, P + L entries (entry i = i % P)
+  qrt::DBuf d_trace_perturb;  // tracer copy of d_perturb, P + L entries
+  qrt::DBuf d_offset_seg;     // heliostats + 1 starts of the per-heliostat offset segments
+  int pool_size = 0;
+  qrt::DBuf d_power, d_diag;
+  std::vector<qm::DevTask> templates;
+  qrt::DBuf d_tasks, d_prefix;
+  std::vector<int> cached_ids;
+  long long cached_lights = -1;
+  bool cache_valid = false;
+  qm::DevTask* h_stage = nullptr;  // pinned staging for task uploads
+  long long* h_prefix = nullptr;
+  size_t stage_cap = 0;
+  cudaEvent_t stage_done = nullptr;
+  qm::SunFrame sun{};
+  int exact = 0;
+  int light_begin = 0, light_end = 0;
+  long long total_facets = 0;
+
+  ~qmcrt_scene() {
+    if (device < 0) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    cudaDeviceSynchronize();
+    if (h_stage) cudaFreeHost(h_stage);
+    if (h_prefix) cudaFreeHost(h_prefix);
+    if (stage_done) cudaEventDestroy(stage_done);
+    grid_bufs.clear();
+    images.clear();
+    d_grids.release();
+    d_receivers.release();
+    d_local.release();
+    d_offsets.release();
+    d_samples.release();
+    d_perturb.release();
+    d_trace_samples.release();
+    d_trace_perturb.release();
+    d_offset_seg.release();
+    d_power.release();
+    d_diag.release();
+    d_tasks.release();
+    d_prefix.release();
+    cudaSetDevice(prev);
+  }
+};
+
+
+namespace qrt {
+
+// Scene helpers defined in capi.cpp.
+void grid_sun_data(const qm::SceneModel& m, const qm::GridModel& g, std::vector<float4>& bound,
+                   std::vector<int4>& hsub, std::vector<float4>& subv);
+qmcrt_scene* checked(qmcrt_scene* s);
+cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st);
+int trace_chunk_rays();
+constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;
+
+}  // namespace qrt

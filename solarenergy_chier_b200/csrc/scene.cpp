@@ -2,6 +2,7 @@
 // Compiled with -ffp-contract=off: the geometry must equal the reference's
 // host computation bit for bit (see scene.h).
 #include "scene.h"
+#include "helio_geom.h"
 
 #include <algorithm>
 #include <cmath>
@@ -332,16 +333,9 @@ float3 focus_center(const ReceiverModel& r, float3 helio_pos) {
 // (FocusFlatRectangleHelio.cu:333-339).
 void orient_heliostat(HeliostatModel& h, float3 focus, float3 sun_dir) {
   if (h.type == 1 && h.focus_length < 0.0f) h.focus_length = length(sub(focus, h.pos));
-  float3 reflect_dir = normalize(sub(focus, h.pos));
-  h.normal = normalize(sub(reflect_dir, sun_dir));
-  const float3 s = h.size;
-  float3* v = h.vertex;
-  v[0] = v3(-s.x / 2, s.y / 2, -s.z / 2);
-  v[1] = add(v3(0, 0, s.z), v[0]);
-  v[2] = add(v3(s.x, 0, s.z), v[0]);
-  v[3] = add(v3(s.x, 0, 0), v[0]);
-  for (int k = 0; k < 4; ++k) v[k] = rotate_to(v[k], h.normal, false);
-  for (int k = 0; k < 4; ++k) v[k] = add(v[k], h.pos);
+  h.focus = focus;
+  h.normal = helio_normal(h.pos, focus, sun_dir);
+  flat_vertices(h.size, h.normal, h.pos, h.vertex);
 }
 
 // Sub-heliostat parallelograms of one heliostat, appended to `out`
@@ -354,11 +348,7 @@ void sub_vertices(HeliostatModel& h, std::vector<float3>& out) {
     return;
   }
   const int rows = h.row_col.x, cols = h.row_col.y;
-  float2 len;
-  len.x = (h.size.z - h.gap.y * (rows - 1)) / float(rows);
-  len.y = (h.size.x - h.gap.x * (cols - 1)) / float(cols);
-  const float3 local[3] = {v3(-len.y / 2, 0.0f, len.x / 2), v3(-len.y / 2, 0.0f, -len.x / 2),
-                           v3(len.y / 2, 0.0f, -len.x / 2)};
+  const float2 len = sub_lengths(h.size, h.gap, h.row_col);
   h.local_centers.assign(rows * cols, v3(0, 0, 0));
   h.local_normals.assign(rows * cols, v3(0, 0, 0));
   if (h.read_method == -1) {
@@ -384,13 +374,9 @@ void sub_vertices(HeliostatModel& h, std::vector<float3>& out) {
     throw std::runtime_error("focus-flat heliostat has no corresponding read method");
   }
   for (int id = 0; id < rows * cols; ++id) {
-    for (int k = 0; k < 3; ++k) {
-      float3 p = rotate_to(local[k], h.local_normals[id], true);
-      p = add(p, h.local_centers[id]);
-      p = rotate_to(p, h.normal, true);
-      p = add(p, h.pos);
-      out.push_back(p);
-    }
+    float3 v[3];
+    focus_flat_sub_vertices(len, h.local_centers[id], h.local_normals[id], h.normal, h.pos, v);
+    out.insert(out.end(), v, v + 3);
   }
 }
 
@@ -684,6 +670,15 @@ bool process_scene(SceneModel& s, std::string& err) {
   } catch (const std::exception& e) {
     err = e.what();
     return false;
+  }
+}
+
+void set_sun(SceneModel& s, float3 sun_dir) {
+  s.config.sun_dir = sun_dir;
+  for (auto& h : s.heliostats) orient_heliostat(h, h.focus, sun_dir);
+  for (auto& g : s.grids) {
+    g.sub_vertices.clear();
+    for (int i = 0; i < g.num_heliostats; ++i) sub_vertices(s.heliostats[g.start_heliostat + i], g.sub_vertices);
   }
 }
 

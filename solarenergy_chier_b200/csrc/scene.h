@@ -70,6 +70,7 @@ struct HeliostatModel {
   float focus_length = -1.f;
   int read_method = -1;
   float pixel_length = 0.f;
+  float3 focus{};                     // aim point on the receiver (sun-independent)
   float3 normal{};
   float3 vertex[4]{};
   int2 sub_row_col{0, 0};
@@ -108,6 +109,12 @@ int read_config_text(const std::string& text, SceneConfig& config, std::string& 
 // QuasiMonteCarloRayTracer::setFlatRectangleHeliostatVertexs
 // (QuasiMonteCarloRayTracing/QuasiMonteCarloRayTracer.cpp:182-209).
 bool process_scene(SceneModel& scene, std::string& err);
+
+// Re-orients every heliostat of a processed scene toward a new sun direction
+// (the sun-dependent half of process_scene: heliostat normals, corner
+// vertices and sub-heliostat parallelograms; aim points, focus lengths, grid
+// cell lists and facet counts do not depend on the sun).
+void set_sun(SceneModel& scene, float3 sun_dir);
 
 // TaskLoader::loadRayTracingHeliostatIndex (RayTracingPipeline/TaskLoader.cpp:114-204).
 // Returns 1 (true), 0 (false: repeated or surplus indexes) or -1 where the

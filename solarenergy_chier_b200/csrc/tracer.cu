@@ -8,7 +8,7 @@
 //
 // Per ray (QuasiMonteCarloRayTracing/RectangleReceiverRectangleGridRayTracing.cu:6-41
 // and CylinderReceiverRectangleGridRayTracing.cu:6-40):
-//   sun sample -> world direction, shadow walk toward the sun, slope-error
+//   world-space sun sample, shadow walk toward the sun, slope-error
 //   normal, reflection, block walk, receiver hit, energy, flux deposit.
 // The walk is the reference's 3D-DDA (QuasiMonteCarloRayTracing/Grid/rectGridDDA.cu:31-119)
 // step for step, including its 1e-5 tie rules and truncating start cell.
@@ -44,7 +44,7 @@ __device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v
 
 // rectGridDDA::absDivide / calTMax / equal / less (rectGridDDA.cuh:15-32).
 __device__ __forceinline__ float abs_divide(float den, float num) {
-  if ((double)num <= kEps && (double)num >= -kEps) return (float)INT_MAX;
+  if (qm_below_eps(num) && qm_above_neg_eps(num)) return (float)INT_MAX;
   return fabsf(den / num);
 }
 __device__ __forceinline__ float cal_tmax(float dir, float interval, int index, float pos) {
@@ -159,14 +159,33 @@ __device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, fl
 // the walk leaves the grid; a walk that stops advancing (an exact tie the
 // reference never leaves) or exceeds cells.x+cells.y+cells.z+2 steps ends
 // here with "no hit" and a diagnostic count instead.
-__device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, float3 d, unsigned& flags) {
-  float3 rel = make_float3(o.x - g.pos.x, o.y - g.pos.y, o.z - g.pos.z);
-  int3 c = trunc3(cdiv(rel, g.interval));
+// Start of a walk from origin o: its cell, and per axis the distances to the
+// cell's lower and upper boundary (rectGridDDA.cu:36-52; calTMax with
+// dir < 0 and dir >= 0).  It depends on the origin only, so both walks of a
+// ray, and every ray of a facet, share it.
+struct WalkStart {
+  int3 cell;
+  float3 lo, hi;
+};
+__device__ __forceinline__ WalkStart walk_start(const DevGrid& g, float3 o) {
+  WalkStart w;
+  const float3 rel = make_float3(o.x - g.pos.x, o.y - g.pos.y, o.z - g.pos.z);
+  w.cell = trunc3(cdiv(rel, g.interval));
+  w.lo = make_float3(cal_tmax(-1.0f, g.interval.x, w.cell.x, rel.x), cal_tmax(-1.0f, g.interval.y, w.cell.y, rel.y),
+                     cal_tmax(-1.0f, g.interval.z, w.cell.z, rel.z));
+  w.hi = make_float3(cal_tmax(1.0f, g.interval.x, w.cell.x, rel.x), cal_tmax(1.0f, g.interval.y, w.cell.y, rel.y),
+                     cal_tmax(1.0f, g.interval.z, w.cell.z, rel.z));
+  return w;
+}
+
+__device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, float3 d, const WalkStart& w,
+                                        unsigned& flags) {
+  int3 c = w.cell;
   int3 st = make_int3(d.x >= 0 ? 1 : -1, d.y >= 0 ? 1 : -1, d.z >= 0 ? 1 : -1);
   float3 tm, td;
-  tm.x = abs_divide(cal_tmax(d.x, g.interval.x, c.x, rel.x), d.x);
-  tm.y = abs_divide(cal_tmax(d.y, g.interval.y, c.y, rel.y), d.y);
-  tm.z = abs_divide(cal_tmax(d.z, g.interval.z, c.z, rel.z), d.z);
+  tm.x = abs_divide(d.x >= 0 ? w.hi.x : w.lo.x, d.x);
+  tm.y = abs_divide(d.y >= 0 ? w.hi.y : w.lo.y, d.y);
+  tm.z = abs_divide(d.z >= 0 ? w.hi.z : w.lo.z, d.z);
   td.x = abs_divide(g.interval.x, d.x);
   td.y = abs_divide(g.interval.y, d.y);
   td.z = abs_divide(g.interval.z, d.z);
@@ -244,7 +263,7 @@ __device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, flo
   float2 ro = make_float2(qm_rn_sub(r.pos.x, o.x), qm_rn_sub(r.pos.z, o.z));
   float tp = qs::dot2(ro, qs::normalize2(make_float2(d.x, d.z)));
   float delta = qm_rn_sub(qs::dot2(ro, ro), qm_rn_mul(tp, tp));
-  if ((double)tp < -kEps || delta > r2) return false;
+  if (qm_below_neg_eps(tp) || delta > r2) return false;
   float t_plus = delta <= 0.0f ? r.size.x : sqrtf(qm_rn_sub(r2, delta));
   t = qm_rn_div(qm_rn_sub(tp, t_plus), qs::length2(make_float2(d.x, d.z)));
   float3 ip = qs::add(qs::mul(d, t), o);
@@ -334,11 +353,43 @@ constexpr int kThreads = QM_TRACE_THREADS;
 constexpr int kWindow = 32;
 
 struct FacetWindow {
-  float4 o[kThreads];  // origin.xyz, pool offset g[f] (int bits)
-  float4 u[kThreads];  // frame u.xyz, pool offset g[(f+1) % P] (int bits)
-  float4 n[kThreads];  // frame n.xyz, frame identity flag
-  float4 v[kThreads];  // frame v.xyz
+  // Per warp: the task's sample pools (P + L entries each, so an offset
+  // g in [0, P) plus a light index in [0, L) needs no wrap-around).
+  const float4* samples[kThreads / 32];
+  const float4* perturbations[kThreads / 32];
+  float4 o[kThreads];   // origin.xyz, pool offset g[f] (int bits)
+  float4 u[kThreads];   // frame u.xyz, pool offset g[(f+1) % P] (int bits)
+  float4 n[kThreads];   // frame n.xyz, frame identity flag
+  float4 v[kThreads];   // frame v.xyz, walk start cell x (int bits)
+  float4 lo[kThreads];  // walk start distances to the lower cell boundaries, cell y
+  float4 hi[kThreads];  // distances to the upper cell boundaries, cell z
 };
+
+// Shared-memory read the compiler may not merge with an earlier read of the
+// same slot: facet data is re-read where it is used instead of being held in
+// registers across a grid walk.
+__device__ __forceinline__ float4 lds(const float4& x) {
+  float4 r;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(&x);
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w) : "r"(a));
+  return r;
+}
+
+__device__ __forceinline__ const float4* lds_ptr(const float4* const& x) {
+  unsigned long long r;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(&x);
+  asm volatile("ld.shared.u64 %0, [%1];" : "=l"(r) : "r"(a));
+  return reinterpret_cast<const float4*>(r);
+}
+
+__device__ __forceinline__ WalkStart window_start(const FacetWindow& win, int slot) {
+  const float4 lo = lds(win.lo[slot]), hi = lds(win.hi[slot]);
+  WalkStart ws;
+  ws.cell = make_int3(__float_as_int(lds(win.v[slot]).w), __float_as_int(lo.w), __float_as_int(hi.w));
+  ws.lo = xyz(lo);
+  ws.hi = xyz(hi);
+  return ws;
+}
 
 template <bool kRecord>
 #ifndef QM_TRACE_MIN_BLOCKS
@@ -369,7 +420,11 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   const DevTask& T = p.tasks[t];
   const DevGrid& G = p.grids[T.grid];
   const DevReceiver& R = p.receivers[T.receiver];
-  const int P = p.pool_size;
+  if (lane == 0) {
+    win.samples[threadIdx.x >> 5] = T.samples;
+    win.perturbations[threadIdx.x >> 5] = T.perturbations;
+  }
+  __syncwarp();
   // This lane's first ray; later rays advance by 32 = q32 * nl + r32.
   int f = (r0 + lane) / nl;
   int l = (r0 + lane) - f * nl;
@@ -396,47 +451,41 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         facet_geometry(T, fw, origin, fnormal);
         const Frame fr = qs::make_frame(fnormal, false);
         win.o[wbase + lane] = make_float4(origin.x, origin.y, origin.z, __int_as_float(__ldg(T.offsets + fw)));
-        win.u[wbase + lane] = make_float4(fr.u.x, fr.u.y, fr.u.z, __int_as_float(__ldg(T.offsets + (fw + 1) % P)));
+        win.u[wbase + lane] = make_float4(fr.u.x, fr.u.y, fr.u.z, __int_as_float(__ldg(T.offsets + (fw + 1) % T.pool_size)));
         win.n[wbase + lane] = make_float4(fr.n.x, fr.n.y, fr.n.z, fr.identity ? 1.0f : 0.0f);
-        win.v[wbase + lane] = make_float4(fr.v.x, fr.v.y, fr.v.z, 0.0f);
+        const WalkStart ws = walk_start(G, origin);
+        win.v[wbase + lane] = make_float4(fr.v.x, fr.v.y, fr.v.z, __int_as_float(ws.cell.x));
+        win.lo[wbase + lane] = make_float4(ws.lo.x, ws.lo.y, ws.lo.z, __int_as_float(ws.cell.y));
+        win.hi[wbase + lane] = make_float4(ws.hi.x, ws.hi.y, ws.hi.z, __int_as_float(ws.cell.z));
       }
       __syncwarp();
     }
     if (active) {
       const int slot = wbase + (f - base);
       const int lab = p.light_begin + l;
-      // Pool offsets lie in [0, P) and light indexes in [0, L), L <= P.
-      int a = __float_as_int(win.o[slot].w) + lab;
-      a -= a >= P ? P : 0;
-      float3 dir = xyz(__ldg(p.samples + a));
-      if (!p.sun.identity) {
-        Frame sun;
-        sun.u = p.sun.u;
-        sun.n = p.sun.n;
-        sun.v = p.sun.v;
-        sun.identity = false;
-        dir = qs::to_world(sun, dir);
-      }
+      // Pool offsets lie in [0, P) and light indexes in [0, L); the pools hold
+      // P + L entries (entry P + i repeats entry i), so (g + l) % P needs no
+      // modulo.  The sun-shape pool is stored already turned by the sun
+      // frame (world space).
+      const float3 dir = xyz(__ldg(lds_ptr(win.samples[threadIdx.x >> 5]) + __float_as_int(win.o[slot].w) + lab));
       int32_t code;
-      if (collide(G, T.own, xyz(win.o[slot]), dir, flags)) {
+      if (collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags)) {
         code = kShadowed;
       } else {
-        int b = __float_as_int(win.u[slot].w) + lab;
-        b -= b >= P ? P : 0;
         Frame nframe;
         nframe.u = xyz(win.u[slot]);
         const float4 wn = win.n[slot];
         nframe.n = xyz(wn);
         nframe.v = xyz(win.v[slot]);
         nframe.identity = wn.w != 0.0f;
-        float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(p.perturbations + b))));
+        const int b = __float_as_int(lds(win.u[slot]).w) + lab;
+        float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
         float3 rd = qs::normalize(qs::reflect(neg(dir), n));
-        const float3 origin = xyz(win.o[slot]);
-        if (collide(G, T.own, origin, rd, flags)) {
+        if (collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags)) {
           code = kBlocked;
         } else {
           float tt, uu, vv;
-          if (!receiver_hit(R, origin, rd, tt, uu, vv)) {
+          if (!receiver_hit(R, xyz(lds(win.o[slot])), rd, tt, uu, vv)) {
             code = kMissed;
           } else {
             float e = qs::ray_energy(tt, rd, n, T.factor);

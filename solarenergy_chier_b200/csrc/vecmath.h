@@ -30,6 +30,18 @@ namespace qm {
 constexpr double kEps = 1e-5;
 }  // namespace qm
 
+// A float compared with the double 1e-5, decided in float.  1e-5f is the
+// largest float below 1e-5 (9.99999974737875e-06; the next float,
+// 1.0000000656873453e-05, lies above it) and no float equals 1e-5, so for
+// every float x (NaN included):
+//   (double)x <  1e-5  <=>  (double)x <= 1e-5  <=>  x <= 1e-5f
+//   (double)x > -1e-5  <=>  (double)x >= -1e-5  <=>  x >= -1e-5f
+//   (double)x < -1e-5  <=>  x < -1e-5f
+// which saves the float-to-double conversions on the device.
+QM_HD bool qm_below_eps(float x) { return x <= 1.0e-5f; }         // (double)x < 1e-5
+QM_HD bool qm_above_neg_eps(float x) { return x >= -1.0e-5f; }    // (double)x > -1e-5
+QM_HD bool qm_below_neg_eps(float x) { return x < -1.0e-5f; }     // (double)x < -1e-5
+
 // Explicitly rounded float operations: on the device the _rn intrinsics,
 // which the compiler never fuses; on the host plain operators (host code is
 // built with -ffp-contract=off).

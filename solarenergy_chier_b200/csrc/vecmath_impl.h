@@ -51,7 +51,7 @@ using Frame = ::qm_frame::Frame;
 QM_HD Frame make_frame(float3 n, bool flip) {
   Frame f;
   f.n = n;
-  f.identity = (double)fabsf(n.x) < kEps && (double)fabsf(n.z) < kEps;
+  f.identity = qm_below_eps(fabsf(n.x)) && qm_below_eps(fabsf(n.z));
   if (f.identity) {
     f.u = make_float3(1.f, 0.f, 0.f);
     f.v = make_float3(0.f, 0.f, 1.f);
@@ -92,7 +92,7 @@ QM_HD bool ray_parallelogram(float3 orig, float3 dir, float3 a, float3 ab, float
                              float& t, float& u, float& v) {
   float3 p = cross(dir, ac);
   float det = dot(ab, p);
-  if ((double)fabsf(det) < kEps) return false;
+  if (qm_below_eps(fabsf(det))) return false;
   float3 tv = sub(orig, a);
   u = QD(dot(tv, p), det);
   if (u < 0 || u > 1) return false;
@@ -100,7 +100,7 @@ QM_HD bool ray_parallelogram(float3 orig, float3 dir, float3 a, float3 ab, float
   v = QD(dot(dir, q), det);
   if (v < 0 || v > 1) return false;
   t = QD(dot(ac, q), det);
-  if ((double)t < kEps) return false;
+  if (qm_below_eps(t)) return false;
   return true;
 }
 

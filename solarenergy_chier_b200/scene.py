@@ -176,6 +176,11 @@ class Scene:
     def set_light_range(self, begin: int, end: int) -> None:
         check(self._lib.qmcrt_set_light_range(self._h, begin, end))
 
+    def set_sun(self, sun_dir) -> None:
+        """Re-orient the field toward a new sun direction (direction of travel)."""
+        d = np.ascontiguousarray(np.asarray(sun_dir, np.float32).reshape(3))
+        check(self._lib.qmcrt_scene_set_sun(self._h, _ptr(d, ctypes.c_float)))
+
     # -- tracing --------------------------------------------------------------
     def trace(self, heliostats, stream=None) -> None:
         ids = np.ascontiguousarray(np.atleast_1d(np.asarray(heliostats, np.int32)))
@@ -231,6 +236,101 @@ class Scene:
         check(self._lib.qmcrt_load_tasks(self._h, str(path).encode(), _ptr(hs, ctypes.c_int), ctypes.byref(nh), cap,
                                          _ptr(rs, ctypes.c_int), ctypes.byref(nr), ctypes.byref(st)))
         return hs[: nh.value].tolist(), rs[: nr.value].tolist(), bool(st.value)
+
+
+class Batch:
+    """Many (scene, sun) instances traced by one launch (qmcrt_batch_*).
+
+    `scenes` is a list of loaded Scenes on one device; `instances` a list of
+    (scene index, sun direction) pairs.  Every instance has its own images and
+    FP64 powers; the sun-dependent geometry is prepared on the GPU."""
+
+    def __init__(self, scenes, instances):
+        lib = load()
+        self._lib = lib
+        self._scenes = list(scenes)  # keep the scenes alive as long as the batch
+        hs = (ctypes.c_void_p * len(self._scenes))(*[s.handle.value for s in self._scenes])
+        idx = np.ascontiguousarray(np.array([int(k) for k, _ in instances], np.int32))
+        suns = np.ascontiguousarray(np.array([np.asarray(d, np.float32) for _, d in instances], np.float32).reshape(-1, 3))
+        self._instances = [(int(k), suns[i]) for i, (k, _) in enumerate(instances)]
+        handle = ctypes.c_void_p()
+        check(lib.qmcrt_batch_create(hs, len(self._scenes), _ptr(idx, ctypes.c_int), _ptr(suns, ctypes.c_float),
+                                     len(self._instances), ctypes.byref(handle)))
+        self._h = handle
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.qmcrt_batch_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def num_instances(self) -> int:
+        return len(self._instances)
+
+    def info(self) -> dict:
+        n, t, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        check(self._lib.qmcrt_batch_info(self._h, ctypes.byref(n), ctypes.byref(t), ctypes.byref(r)))
+        return {"instances": n.value, "tasks": t.value, "rays_per_trace": r.value}
+
+    def set_suns(self, sun_dirs, stream=None) -> None:
+        d = np.ascontiguousarray(np.asarray(sun_dirs, np.float32).reshape(-1, 3))
+        if d.shape[0] != self.num_instances:
+            raise ValueError("one sun direction per instance")
+        check(self._lib.qmcrt_batch_set_suns(self._h, _ptr(d, ctypes.c_float), _stream_handle(stream)))
+
+    def set_light_range(self, begin: int, end: int) -> None:
+        check(self._lib.qmcrt_batch_set_light_range(self._h, begin, end))
+
+    def set_math_mode(self, mode) -> None:
+        check(self._lib.qmcrt_batch_set_math_mode(self._h, int(mode)))
+
+    def trace(self, stream=None) -> None:
+        check(self._lib.qmcrt_batch_trace(self._h, _stream_handle(stream)))
+
+    def capture_graph(self, clear_first: bool = True) -> None:
+        check(self._lib.qmcrt_batch_capture_graph(self._h, int(bool(clear_first))))
+
+    def graph_launch(self, stream=None) -> None:
+        check(self._lib.qmcrt_batch_graph_launch(self._h, _stream_handle(stream)))
+
+    def clear(self, stream=None) -> None:
+        check(self._lib.qmcrt_batch_clear(self._h, _stream_handle(stream)))
+
+    def autotune(self, stream=None) -> tuple[int, float]:
+        m, ms = ctypes.c_int(), ctypes.c_float()
+        check(self._lib.qmcrt_batch_autotune(self._h, _stream_handle(stream), ctypes.byref(m), ctypes.byref(ms)))
+        return m.value, ms.value
+
+    def image(self, instance: int, receiver: int = 0) -> np.ndarray:
+        w, h = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.qmcrt_batch_image(self._h, instance, receiver, None, ctypes.byref(w), ctypes.byref(h)))
+        out = np.zeros((h.value, w.value), np.float32)
+        check(self._lib.qmcrt_batch_image(self._h, instance, receiver, _ptr(out, ctypes.c_float), ctypes.byref(w),
+                                          ctypes.byref(h)))
+        return out
+
+    def geometry(self, instance: int, grid: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """Device-prepared sub-heliostat vertices of one grid and heliostat normals."""
+        s = self._scenes[self._instances[instance][0]]
+        g = s.grid(grid)
+        verts = np.zeros((g["num_sub"] * 3, 3), np.float32)
+        normals = np.zeros((s.num_heliostats, 3), np.float32)
+        check(self._lib.qmcrt_batch_debug_geometry(self._h, instance, grid, _ptr(verts, ctypes.c_float),
+                                                   _ptr(normals, ctypes.c_float)))
+        return verts, normals
+
+    def power(self, instance: int) -> tuple[np.ndarray, float]:
+        k = self._instances[instance][0]
+        per = np.zeros(self._scenes[k].num_heliostats, np.float64)
+        total = ctypes.c_double()
+        check(self._lib.qmcrt_batch_power_fp64(self._h, instance, _ptr(per, ctypes.c_double), ctypes.byref(total)))
+        return per, total.value
 
 
 def smooth_device(device_ptr: int, width: int, height: int, radius: int, ratio: float, stream=None) -> None:

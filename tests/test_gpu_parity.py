@@ -269,3 +269,27 @@ def test_fp64_accuracy_of_production_path(large):
     got = s.hit_records(ids[-1], 0, 300, 0, L)
     w64 = o64.trace([ids[-1]], large.dirs, large.pert, large.offsets, record=(ids[-1], 0, 300), images=False)["records"]
     assert np.mean((got >= 0) == (w64 >= 0)) >= 0.999
+
+
+def test_set_sun_traces_like_a_scene_loaded_with_that_sun(tmp_path):
+    # qmcrt_scene_set_sun on the device: per-ray outcomes equal the oracle's
+    # for a configuration holding the new sun (exact math mode).
+    import json
+    from pathlib import Path
+
+    f = synth.large_field(tmp_path, seed=6, num_heliostats=24, helio_pixel=0.25, receiver_pixel=0.05, groups=4,
+                          per_group=128)
+    c = Case(f, seed=9)
+    sun = [0.35, -0.75, 0.56]
+    cfg = json.loads(Path(f.config).read_text())
+    c2 = tmp_path / "sun2.json"
+    c2.write_text(json.dumps(dict(cfg, sun_dir=sun)))
+    o2 = oracle.OracleScene.from_files(f.scene, c2)
+    c.scene.set_sun(sun)
+    c.scene.set_math_mode(True)
+    L = c.scene.lights_per_group
+    for h in (0, 11, 23):
+        nf = c.scene.heliostat(h)["num_facets"]
+        got = c.scene.hit_records(h, 0, min(nf, 200), 0, L)
+        want = o2.trace([h], c.dirs, c.pert, c.offsets, record=(h, 0, min(nf, 200)), images=False)["records"]
+        assert np.array_equal(got, want), f"heliostat {h}: {np.mean(got != want):.2e} of rays differ"

@@ -230,6 +230,23 @@ def test_geometry_synthetic_large(tmp_path):
     assert p.receiver(0)["width"] == 1257 and p.receiver(0)["height"] == 600
 
 
+def test_set_sun_equals_loading_with_that_sun(tmp_path):
+    # qmcrt_scene_set_sun re-runs the sun-dependent half of processScene: the
+    # re-oriented field must equal, bit for bit, a field loaded with that sun
+    # in its configuration (and therefore the oracle's).
+    import json
+
+    f = synth.large_field(tmp_path, seed=4, num_heliostats=40, helio_pixel=0.25)
+    cfg = json.loads(Path(f.config).read_text())
+    for sun in ([0.3, -0.8, 0.52], [-0.1, -0.95, -0.3]):
+        cfg2 = dict(cfg, sun_dir=sun)
+        c2 = tmp_path / f"cfg_{sun[0]}.json"
+        c2.write_text(json.dumps(cfg2))
+        moved = load_host(f.scene, f.config)
+        moved.set_sun(sun)
+        assert_same_geometry(moved, oracle.OracleScene.from_files(f.scene, c2))
+
+
 def test_geometry_full_large_field_counts(tmp_path):
     f = synth.large_field(tmp_path)
     p = load_host(f.scene, f.config)
