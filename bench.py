@@ -20,6 +20,12 @@ Multi-GPU (torchrun): every rank traces the full field for its own light
 ranges (weak scaling, no collective inside the timed region); time is the
 maximum over ranks.
 
+`batched` (--batched-lights, default 4 light indexes per sun) compares, over
+96 sun positions (12 days x 8 hours, elevations 15-80 deg), the plain path
+looped over the suns with one batch traced by a single CUDA-graph launch.
+`reference_cuda` (--reference-cuda N) times the reference's own CUDA build
+on N heliostats spread over the field, and this tracer on the same ones.
+
 --impl reference times the reference's own per-ray routine (its host code
 compiled from the reference tree, OpenMP over all host cores) on a bounded
 sample of the same workload.
@@ -52,6 +58,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--passes", type=int, default=32, help="light indexes per step")
+    p.add_argument("--batched-lights", type=int, default=4,
+                   help="light indexes per sun of the 96-sun batched-vs-plain comparison (0 = skip)")
     p.add_argument("--impl", default="native", choices=["native", "reference"])
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -151,6 +159,71 @@ def census(files, lights: int = 8, stride: int = 4001):
                     + 20 * per["cells"] + 70 + 55 * reach_receiver)
     per["rays_sampled"] = n
     return per
+
+
+def batched_vs_plain(torch, scene, lights: int, stream):
+    """96 sun positions (12 days x 8 hours) of the field, `lights` light
+    indexes per facet per sun: the plain path looped over the suns (set_sun,
+    clear, one trace launch, image + FP64 power read back per sun) against one
+    batch (device-side preparation of all suns, one CUDA-graph launch that
+    clears and traces every sun, the same read-backs).  CUDA events on one
+    stream around each whole loop; the scene's own sun is restored after."""
+    import numpy as np
+
+    import solarenergy_chier_b200 as q
+    from solarenergy_chier_b200 import synth
+
+    suns = synth.sun_positions()
+    own_sun = np.array(scene.info.sun_dir[:], np.float32)
+    ids = list(range(scene.num_heliostats))
+    nf = sum(scene.heliostat(h)["num_facets"] for h in ids)
+    rays = nf * lights * len(suns)
+    scene.set_light_range(0, lights)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def plain_loop(sun_list):
+        for sun in sun_list:
+            scene.set_sun(sun)
+            scene.clear(stream=stream)
+            scene.clear_power()
+            scene.trace(ids, stream)
+            scene.image(0)
+            scene.power()
+
+    plain_loop(suns[:2])  # warm-up
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plain_loop(suns)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+
+    batch = q.Batch([scene], [(0, s) for s in suns])
+    batch.set_light_range(0, lights)
+    mode, _ = batch.autotune(stream)
+    batch.capture_graph(clear_first=True)
+    batch.graph_launch(stream)  # warm-up
+    torch.cuda.synchronize()
+    e0.record(stream)
+    batch.set_suns(suns, stream)
+    batch.graph_launch(stream)
+    for k in range(len(suns)):
+        batch.image(k)
+        batch.power(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_ms = e0.elapsed_time(e1)
+    e0.record(stream)
+    batch.graph_launch(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    kernel_ms = e0.elapsed_time(e1)
+    batch.close()
+    scene.set_sun(own_sun)
+    return {"suns": len(suns), "lights_per_sun": lights, "rays": rays, "autotuned_mode": mode,
+            "plain_looped_mrays_s": rays / (plain_ms / 1e3) / 1e6, "batched_mrays_s": rays / (batched_ms / 1e3) / 1e6,
+            "batched_graph_only_mrays_s": rays / (kernel_ms / 1e3) / 1e6,
+            "speedup_batched_vs_plain": plain_ms / batched_ms, "plain_ms": plain_ms, "batched_ms": batched_ms}
 
 
 def cpu_baseline(files, seconds: float):
@@ -358,6 +431,8 @@ def main():
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps},
                 "roofline": roofline}
+        if args.batched_lights > 0:
+            line["batched"] = batched_vs_plain(torch, scene, args.batched_lights, stream)
         if args.reference_cuda > 0:
             line["reference_cuda"] = reference_cuda(files, scene, args.reference_cuda)
         if not args.no_cpu_baseline:

@@ -18,55 +18,11 @@
 #include <string>
 #include <vector>
 
-#include "prep.h"
-#include "runtime.h"
+#include "batch_state.h"
 #include "tracer.h"
 #include "vecmath.h"
 
 using namespace qrt;
-
-struct qmcrt_batch {
-  int device = 0;
-  struct Instance {
-    qmcrt_scene* scene;
-    float3 sun;
-    int grid_base, recv_base, power_base, task_base;
-    long long pool_base;   // first float4 of its world-space pool (P + L entries)
-  };
-  std::vector<Instance> inst;
-  std::vector<long long> image_offset;  // per instance-receiver, into d_images
-  std::vector<int2> image_shape;        // (width, height)
-  std::vector<qm::DevGrid> grids;
-  std::vector<qm::DevReceiver> receivers;
-  std::vector<qm::DevTask> tasks;
-  std::vector<qm::PrepItem> items;
-  DBuf d_grids, d_receivers, d_tasks, d_prefix, d_items, d_rot;
-  DBuf d_bound, d_hsub, d_subv, d_verts;  // per instance-grid slices
-  DBuf d_images, d_power, d_diag, d_pools;
-  int light_begin = 0, light_end = 0, max_lights = 0;
-  long long total_chunks = -1;  // for the current light range; -1 = prefix not built
-  int mode = 0;                 // 0 production, 1 exact, 2 production 48 registers
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-
-  void drop_graph() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
-    if (graph) cudaGraphDestroy(graph);
-    graph_exec = nullptr;
-    graph = nullptr;
-  }
-  ~qmcrt_batch() {
-    int prev = 0;
-    cudaGetDevice(&prev);
-    cudaSetDevice(device);
-    cudaDeviceSynchronize();
-    drop_graph();
-    for (DBuf* b : {&d_grids, &d_receivers, &d_tasks, &d_prefix, &d_items, &d_rot, &d_bound, &d_hsub, &d_subv,
-                    &d_verts, &d_images, &d_power, &d_diag, &d_pools})
-      b->release();
-    cudaSetDevice(prev);
-  }
-};
 
 namespace {
 
@@ -93,8 +49,11 @@ qm::SunFrame sun_frame(float3 sun) {
   return s;
 }
 
-// Device preparation of every instance for its current sun.
-void prepare(qmcrt_batch* b, cudaStream_t st) {
+}  // namespace
+
+namespace qrt {
+
+void batch_prepare(qmcrt_batch* b, cudaStream_t st) {
   for (size_t k = 0; k < b->inst.size(); ++k) {
     const auto& I = b->inst[k];
     const int H = (int)I.scene->model.heliostats.size();
@@ -128,7 +87,7 @@ void prepare(qmcrt_batch* b, cudaStream_t st) {
   cuda_check(cudaStreamSynchronize(st), "batch preparation");
 }
 
-void build_prefix(qmcrt_batch* b) {
+void batch_build_prefix(qmcrt_batch* b) {
   const long long nl = b->light_end - b->light_begin;
   const long long chunk = trace_chunk_rays();
   std::vector<long long> prefix(b->tasks.size() + 1, 0);
@@ -141,7 +100,7 @@ void build_prefix(qmcrt_batch* b) {
   b->total_chunks = prefix.back();
 }
 
-cudaError_t launch(qmcrt_batch* b, cudaStream_t st) {
+cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out) {
   qm::TraceParams p{};
   p.grids = b->d_grids.as<qm::DevGrid>();
   p.receivers = b->d_receivers.as<qm::DevReceiver>();
@@ -154,11 +113,15 @@ cudaError_t launch(qmcrt_batch* b, cudaStream_t st) {
   p.power = b->d_power.as<double>();
   p.diag = b->d_diag.as<unsigned long long>();
   switch (b->mode) {
-    case 1: return qm::launch_trace_exact(p, false, st);
-    case 2: return qm::launch_trace_fast4(p, false, st);
-    default: return qm::launch_trace_fast(p, false, st);
+    case 1: return qm::launch_trace_exact(p, out, st);
+    case 2: return qm::launch_trace_fast4(p, out, st);
+    default: return qm::launch_trace_fast(p, out, st);
   }
 }
+
+}  // namespace qrt
+
+namespace {
 
 void clear_async(qmcrt_batch* b, cudaStream_t st) {
   cuda_check(cudaMemsetAsync(b->d_images.p, 0, b->d_images.bytes, st), "clear");
@@ -283,7 +246,7 @@ int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scen
     b->d_items.alloc(b->items.size() * sizeof(qm::PrepItem));
     b->light_begin = 0;
     b->light_end = b->max_lights;
-    prepare(b.get(), 0);
+    batch_prepare(b.get(), 0);
     *out = b.release();
   });
 }
@@ -296,7 +259,7 @@ int qmcrt_batch_set_suns(qmcrt_batch* b, const float* sun_dirs, void* stream) {
     if (!sun_dirs) invalid("sun directions are NULL");
     for (size_t k = 0; k < b->inst.size(); ++k) b->inst[k].sun = sun_of(sun_dirs, (int)k);
     DeviceGuard guard(b->device);
-    prepare(b, static_cast<cudaStream_t>(stream));
+    batch_prepare(b, static_cast<cudaStream_t>(stream));
   });
 }
 
@@ -338,8 +301,8 @@ int qmcrt_batch_trace(qmcrt_batch* b, void* stream) {
     batch_checked(b);
     if (b->light_end == b->light_begin) return;
     DeviceGuard guard(b->device);
-    if (b->total_chunks < 0) build_prefix(b);
-    cuda_check(launch(b, static_cast<cudaStream_t>(stream)), "batch trace");
+    if (b->total_chunks < 0) batch_build_prefix(b);
+    cuda_check(batch_launch(b, static_cast<cudaStream_t>(stream), 0), "batch trace");
   });
 }
 
@@ -347,7 +310,7 @@ int qmcrt_batch_capture_graph(qmcrt_batch* b, int clear_first) {
   return guarded([&] {
     batch_checked(b);
     DeviceGuard guard(b->device);
-    if (b->total_chunks < 0) build_prefix(b);
+    if (b->total_chunks < 0) batch_build_prefix(b);
     b->drop_graph();
     cudaStream_t st;
     cuda_check(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -357,7 +320,7 @@ int qmcrt_batch_capture_graph(qmcrt_batch* b, int clear_first) {
         cudaMemsetAsync(b->d_images.p, 0, b->d_images.bytes, st);
         cudaMemsetAsync(b->d_power.p, 0, b->d_power.bytes, st);
       }
-      if (b->light_end > b->light_begin) launch(b, st);
+      if (b->light_end > b->light_begin) batch_launch(b, st, 0);
       cudaError_t e2 = cudaStreamEndCapture(st, &b->graph);
       e = e2;
     }
@@ -464,7 +427,7 @@ int qmcrt_batch_autotune(qmcrt_batch* b, void* stream, int* chosen, float* ms) {
   return guarded([&] {
     batch_checked(b);
     DeviceGuard guard(b->device);
-    if (b->total_chunks < 0) build_prefix(b);
+    if (b->total_chunks < 0) batch_build_prefix(b);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // Candidates give identical results (same arithmetic, different register
     // budgets and occupancy); time each on the batch itself and keep the
@@ -477,9 +440,9 @@ int qmcrt_batch_autotune(qmcrt_batch* b, void* stream, int* chosen, float* ms) {
     int pick = 0;
     for (int c : candidates) {
       b->mode = c;
-      cuda_check(launch(b, st), "autotune");  // warm-up
+      cuda_check(batch_launch(b, st, 0), "autotune");  // warm-up
       cudaEventRecord(e0, st);
-      cuda_check(launch(b, st), "autotune");
+      cuda_check(batch_launch(b, st, 0), "autotune");
       cudaEventRecord(e1, st);
       cuda_check(cudaEventSynchronize(e1), "autotune");
       float t = 0.f;

@@ -81,6 +81,8 @@ struct TraceParams {
   int lights_q32, lights_r32;     // 32 / (light_end - light_begin) and 32 % it (set by the launcher)
   double* power;                  // FP64 per-slot power accumulators
   unsigned long long* diag;
+  // bilinear-deposit variant only: one word per warp iteration, bit i = lane i's ray hit the receiver
+  uint32_t* hit_bits;
   // hit-record variant only
   int32_t* records;
   int record_task;

@@ -22,7 +22,15 @@ __global__ void prep_kernel(const PrepItem* items, int n, DevTask* tasks) {
   if (i >= n) return;
   const PrepItem it = items[i];
   DevTask& T = tasks[it.task];
-  const float3 normal = helio_normal(T.pos, it.focus, it.sun_dir);
+  float3 aim = it.focus;
+  if (it.aim_offset.x != 0.0f || it.aim_offset.y != 0.0f)
+    aim = qs::add(qs::add(aim, qs::mul(it.aim_u, it.aim_offset.x)), qs::mul(it.aim_v, it.aim_offset.y));
+  float3 normal = helio_normal(T.pos, aim, it.sun_dir);
+  if (it.normal_offset.x != 0.0f || it.normal_offset.y != 0.0f) {
+    const Frame f0 = qs::make_frame(normal, false);
+    normal = qs::normalize(
+        qs::add(qs::add(normal, qs::mul(f0.u, it.normal_offset.x)), qs::mul(f0.v, it.normal_offset.y)));
+  }
   T.normal = normal;
   const Frame hf = qs::make_frame(normal, T.type == 1);
   T.fu = hf.u;

@@ -17,6 +17,11 @@ struct PrepItem {
   int sub_first;    // grid-local id of its first sub-heliostat
   float3 focus;     // aim point (sun-independent)
   float3 sun_dir;   // direction of travel of the sun's rays
+  // Differentiable parameters (zero for plain batches): the aim point moves
+  // by aim_offset.x * aim_u + aim_offset.y * aim_v; the normal then turns by
+  // normal_offset (radians) about the u and v axes of its own frame.
+  float2 aim_offset, normal_offset;
+  float3 aim_u, aim_v;
   float3* verts;    // out: 3 float3 (B, A, C) per sub-heliostat
   float4* subv;     // out: 3 float4 per sub-heliostat (A, B - A, C - A)
   float4* bound;    // out: 5 float4 traversal record

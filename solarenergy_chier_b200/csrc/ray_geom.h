@@ -1,0 +1,97 @@
+// Device geometry of one ray outside the grid walk, shared by the tracer
+// (tracer.cu) and the differentiable forward / adjoint (diff.cu): the
+// micro-facet of a task, the receiver intersections and the task lookup.
+// Every operation is explicitly rounded (qs::), so results do not depend on
+// the unit's FMA contraction setting and equal the CPU oracle's.
+#pragma once
+
+#include <climits>
+
+#include "device_scene.h"
+#include "vecmath.h"
+
+namespace qm {
+
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+
+// CylinderReceiver::GIntersect (Scene/DataStructure/Receiver/CylinderReceiver.cuh:39-89),
+// every operation explicitly rounded: delta = |Ro|^2 - tp^2 cancels
+// catastrophically for far heliostats (|Ro|^2 ~ 5e5 m^2, float spacing
+// 0.03 m^2), so a fused multiply-add there would move rays across the
+// cylinder's silhouette relative to the reference's rounding.
+// acos takes its argument clamped to [-1, 1]; the reference prints an error
+// and lets a NaN through when rounding pushes it outside.
+__device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
+  float2 l = make_float2(qm_rn_sub(o.x, r.pos.x), qm_rn_sub(o.z, r.pos.z));
+  const float r2 = qm_rn_mul(r.size.x, r.size.x);
+  if (qs::dot2(l, l) <= r2) return false;
+  float2 ro = make_float2(qm_rn_sub(r.pos.x, o.x), qm_rn_sub(r.pos.z, o.z));
+  float tp = qs::dot2(ro, qs::normalize2(make_float2(d.x, d.z)));
+  float delta = qm_rn_sub(qs::dot2(ro, ro), qm_rn_mul(tp, tp));
+  if (qm_below_neg_eps(tp) || delta > r2) return false;
+  float t_plus = delta <= 0.0f ? r.size.x : sqrtf(qm_rn_sub(r2, delta));
+  t = qm_rn_div(qm_rn_sub(tp, t_plus), qs::length2(make_float2(d.x, d.z)));
+  float3 ip = qs::add(qs::mul(d, t), o);
+  u = qm_rn_add(qm_rn_div(qm_rn_sub(ip.y, r.pos.y), r.size.y), 0.5f);
+  if (u < 0.0f || u > 1.0f) return false;
+  float2 cs = qs::normalize2(make_float2(qm_rn_sub(ip.x, r.pos.x), qm_rn_sub(ip.z, r.pos.z)));
+  float cx = fminf(fmaxf(cs.x, -1.0f), 1.0f);
+  v = (float)__ddiv_rn((double)acosf(cx), 2 * M_PI);
+  if (cs.y < 0) v = qm_rn_sub(1.0f, v);
+  return true;
+}
+
+__device__ __forceinline__ bool receiver_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
+  if (r.type == 0) return qs::ray_parallelogram(o, d, r.a, r.ab, r.ac, t, u, v);
+  return cylinder_hit(r, o, d, t, u, v);
+}
+
+// Micro-facet centre and normal (rectangle_heliostat::map_microhelio_center_and_normal,
+// Scene/DataStructure/Heliostat/RectangleHelio.cu:54-80; focusFlatRectangle_heliostat
+// kernels, FocusFlatRectangleHelio.cu:12-64), evaluated per facet instead of
+// materialised; explicitly rounded (once per facet, off the hot path).
+__device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& origin, float3& normal) {
+  Frame hf;
+  hf.u = T.fu;
+  hf.n = T.fn;
+  hf.v = T.fv;
+  hf.identity = T.frame_identity != 0;
+  const int per_row = T.row_col.y * T.sub_row_col.y;
+  int row = f / per_row;
+  int col = f % per_row;
+  const float px = T.pixel_length;
+  if (T.type == 0) {
+    int brow = row / T.sub_row_col.x;
+    int bcol = col / T.sub_row_col.y;
+    float3 c;
+    c.x = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)col, px), qm_rn_mul((float)bcol, T.gap.x)), px / 2),
+                    T.size.x / 2);
+    c.y = T.size.y / 2;
+    c.z = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)row, px), qm_rn_mul((float)brow, T.gap.y)), px / 2),
+                    T.size.z / 2);
+    origin = qs::add(qs::to_world(hf, c), T.pos);
+    normal = T.normal;
+  } else {
+    int block = (row / T.sub_row_col.x) * T.row_col.y + col / T.sub_row_col.y;
+    float3 ln = T.local_normals[block];
+    float3 lc = T.local_centers[block];
+    row %= T.sub_row_col.x;
+    col %= T.sub_row_col.y;
+    float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)col, 0.5f), px), T.sub_length.y / 2), 0.0f,
+                            qm_rn_sub(qm_rn_mul(qm_rn_add((float)row, 0.5f), px), T.sub_length.x / 2));
+    lp = qs::add(qs::rotate_to(lp, ln, true), lc);
+    normal = qs::to_world(hf, ln);
+    origin = qs::add(qs::to_world(hf, lp), T.pos);
+  }
+}
+
+__device__ __forceinline__ int find_task(const long long* prefix, int n, long long w) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (__ldg(prefix + mid) <= w) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+}  // namespace qm

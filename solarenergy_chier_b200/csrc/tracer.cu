@@ -27,6 +27,7 @@
 #include <climits>
 
 #include "device_scene.h"
+#include "ray_geom.h"
 #include "tracer.h"
 #include "vecmath.h"
 
@@ -39,8 +40,6 @@
 
 namespace qm {
 namespace {
-
-__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
 
 // rectGridDDA::absDivide / calTMax / equal / less (rectGridDDA.cuh:15-32).
 __device__ __forceinline__ float abs_divide(float den, float num) {
@@ -249,86 +248,6 @@ __device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, flo
   return false;
 }
 
-// CylinderReceiver::GIntersect (Scene/DataStructure/Receiver/CylinderReceiver.cuh:39-89),
-// every operation explicitly rounded: delta = |Ro|^2 - tp^2 cancels
-// catastrophically for far heliostats (|Ro|^2 ~ 5e5 m^2, float spacing
-// 0.03 m^2), so a fused multiply-add there would move rays across the
-// cylinder's silhouette relative to the reference's rounding.
-// acos takes its argument clamped to [-1, 1]; the reference prints an error
-// and lets a NaN through when rounding pushes it outside.
-__device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
-  float2 l = make_float2(qm_rn_sub(o.x, r.pos.x), qm_rn_sub(o.z, r.pos.z));
-  const float r2 = qm_rn_mul(r.size.x, r.size.x);
-  if (qs::dot2(l, l) <= r2) return false;
-  float2 ro = make_float2(qm_rn_sub(r.pos.x, o.x), qm_rn_sub(r.pos.z, o.z));
-  float tp = qs::dot2(ro, qs::normalize2(make_float2(d.x, d.z)));
-  float delta = qm_rn_sub(qs::dot2(ro, ro), qm_rn_mul(tp, tp));
-  if (qm_below_neg_eps(tp) || delta > r2) return false;
-  float t_plus = delta <= 0.0f ? r.size.x : sqrtf(qm_rn_sub(r2, delta));
-  t = qm_rn_div(qm_rn_sub(tp, t_plus), qs::length2(make_float2(d.x, d.z)));
-  float3 ip = qs::add(qs::mul(d, t), o);
-  u = qm_rn_add(qm_rn_div(qm_rn_sub(ip.y, r.pos.y), r.size.y), 0.5f);
-  if (u < 0.0f || u > 1.0f) return false;
-  float2 cs = qs::normalize2(make_float2(qm_rn_sub(ip.x, r.pos.x), qm_rn_sub(ip.z, r.pos.z)));
-  float cx = fminf(fmaxf(cs.x, -1.0f), 1.0f);
-  v = (float)__ddiv_rn((double)acosf(cx), 2 * M_PI);
-  if (cs.y < 0) v = qm_rn_sub(1.0f, v);
-  return true;
-}
-
-__device__ __forceinline__ bool receiver_hit(const DevReceiver& r, float3 o, float3 d, float& t, float& u, float& v) {
-  if (r.type == 0) return qs::ray_parallelogram(o, d, r.a, r.ab, r.ac, t, u, v);
-  return cylinder_hit(r, o, d, t, u, v);
-}
-
-// Micro-facet centre and normal (rectangle_heliostat::map_microhelio_center_and_normal,
-// Scene/DataStructure/Heliostat/RectangleHelio.cu:54-80; focusFlatRectangle_heliostat
-// kernels, FocusFlatRectangleHelio.cu:12-64), evaluated per facet instead of
-// materialised; explicitly rounded (once per facet, off the hot path).
-__device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& origin, float3& normal) {
-  Frame hf;
-  hf.u = T.fu;
-  hf.n = T.fn;
-  hf.v = T.fv;
-  hf.identity = T.frame_identity != 0;
-  const int per_row = T.row_col.y * T.sub_row_col.y;
-  int row = f / per_row;
-  int col = f % per_row;
-  const float px = T.pixel_length;
-  if (T.type == 0) {
-    int brow = row / T.sub_row_col.x;
-    int bcol = col / T.sub_row_col.y;
-    float3 c;
-    c.x = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)col, px), qm_rn_mul((float)bcol, T.gap.x)), px / 2),
-                    T.size.x / 2);
-    c.y = T.size.y / 2;
-    c.z = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)row, px), qm_rn_mul((float)brow, T.gap.y)), px / 2),
-                    T.size.z / 2);
-    origin = qs::add(qs::to_world(hf, c), T.pos);
-    normal = T.normal;
-  } else {
-    int block = (row / T.sub_row_col.x) * T.row_col.y + col / T.sub_row_col.y;
-    float3 ln = T.local_normals[block];
-    float3 lc = T.local_centers[block];
-    row %= T.sub_row_col.x;
-    col %= T.sub_row_col.y;
-    float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)col, 0.5f), px), T.sub_length.y / 2), 0.0f,
-                            qm_rn_sub(qm_rn_mul(qm_rn_add((float)row, 0.5f), px), T.sub_length.x / 2));
-    lp = qs::add(qs::rotate_to(lp, ln, true), lc);
-    normal = qs::to_world(hf, ln);
-    origin = qs::add(qs::to_world(hf, lp), T.pos);
-  }
-}
-
-__device__ __forceinline__ int find_task(const long long* prefix, int n, long long w) {
-  int lo = 0, hi = n - 1;
-  while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (__ldg(prefix + mid) <= w) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
 // Rays of one launch: for task t (a heliostat), rays r in [0, F_t * nl) with
 // facet f = r / nl and light l = light_begin + r % nl, nl = lights per facet.
 // Each warp takes one chunk of kChunk consecutive rays of one task (task ray
@@ -391,7 +310,32 @@ __device__ __forceinline__ WalkStart window_start(const FacetWindow& win, int sl
   return ws;
 }
 
-template <bool kRecord>
+// Output of a launch: flux into the receiver images (nearest pixel, the
+// reference's deposit), per-ray outcome codes, or the differentiable
+// forward's bilinear deposit plus one hit bit per ray.
+enum TraceOut { kOutFlux = 0, kOutRecord = 1, kOutSplat = 2 };
+
+// Bilinear deposit of energy e at continuous pixel position (X, Y) (pixel c
+// spans [c, c+1), centres at c + 0.5): columns wrap around for a cylinder
+// (its columns are angles), everything else outside the image is dropped.
+__device__ __forceinline__ void splat_bilinear(const DevReceiver& R, float X, float Y, float e) {
+  const float x = X - 0.5f, y = Y - 0.5f;
+  const float x0 = floorf(x), y0 = floorf(y);
+  const float fx = x - x0, fy = y - y0;
+  const int c0 = (int)x0, r0 = (int)y0;
+  const int w = R.resolution.x, h = R.resolution.y;
+  const bool wrap = R.type == 1;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    int c = c0 + (k & 1), r = r0 + (k >> 1);
+    const float wgt = ((k & 1) ? fx : 1.0f - fx) * ((k >> 1) ? fy : 1.0f - fy);
+    if (wrap) c = c < 0 ? c + w : (c >= w ? c - w : c);
+    if (c < 0 || c >= w || r < 0 || r >= h) continue;
+    atomicAdd(R.image + r * w + c, e * wgt);
+  }
+}
+
+template <int kOut>
 #ifndef QM_TRACE_MIN_BLOCKS
 #define QM_TRACE_MIN_BLOCKS 4
 #endif
@@ -404,7 +348,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   // Ray indexes within one heliostat fit in int: the host refuses launches
   // with num_facets * lights >= 2^31.
   int t, r0, r_end;
-  if (kRecord) {
+  if (kOut == kOutRecord) {
     const long long span = (long long)(p.record_facet_end - p.record_facet_begin) * nl;
     if (warp * kChunk >= span) return;
     t = p.record_task;
@@ -438,6 +382,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   bool filled = false;  // warp-uniform
   for (int it = 0; it < iters; ++it) {
     const bool active = r0 + it * 32 + lane < r_end;
+    bool hit = false;
     // Lane 0 holds the smallest facet of the iteration (it is active whenever
     // any lane is) and every facet of the iteration lies within 31 of it.
     const int f0 = __shfl_sync(0xffffffffu, f, 0);
@@ -489,6 +434,11 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
             code = kMissed;
           } else {
             float e = qs::ray_energy(tt, rd, n, T.factor);
+            if (kOut == kOutSplat) {
+              splat_bilinear(R, qm_rn_mul(vv, (float)R.resolution.x), qm_rn_mul(uu, (float)R.resolution.y), e);
+              power += (double)e;
+              code = 0;
+            } else {
             int row = int(qm_rn_mul(uu, (float)R.resolution.y));
             int col = int(qm_rn_mul(vv, (float)R.resolution.x));
             if (row >= R.resolution.y || col >= R.resolution.x || row < 0 || col < 0) {
@@ -500,10 +450,16 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
             atomicAdd(R.image + pix, e);
             power += (double)e;
             code = pix;
+            }
           }
         }
       }
-      if (kRecord) p.records[(size_t)(f - p.record_facet_begin) * nl + l] = code;
+      if (kOut == kOutRecord) p.records[(size_t)(f - p.record_facet_begin) * nl + l] = code;
+      if (kOut == kOutSplat) hit = code >= 0;
+    }
+    if (kOut == kOutSplat) {
+      const unsigned bits = __ballot_sync(0xffffffffu, hit);
+      if (lane == 0) p.hit_bits[warp * kChunkIters + it] = bits;
     }
     f += q32;
     l += r32;
@@ -544,22 +500,24 @@ cudaError_t QM_SYM(launch_facets)(const DevTask& task, float3* origins, float3* 
 
 int QM_SYM(trace_chunk_rays)() { return kChunk; }
 
-cudaError_t QM_SYM(launch_trace)(const TraceParams& params, bool record, cudaStream_t stream) {
+cudaError_t QM_SYM(launch_trace)(const TraceParams& params, int out, cudaStream_t stream) {
   const int threads = kThreads;
   const long long nl = params.light_end - params.light_begin;
   if (nl <= 0) return cudaSuccess;
   TraceParams p = params;
   p.lights_q32 = (int)(32 / nl);
   p.lights_r32 = (int)(32 % nl);
+  const bool record = out == kOutRecord;
   const long long warps = record ? ((long long)(p.record_facet_end - p.record_facet_begin) * nl + kChunk - 1) / kChunk
                                  : p.total_facets;
   if (warps <= 0) return cudaSuccess;
   const long long blocks = (warps + (threads / 32) - 1) / (threads / 32);
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-  if (record)
-    trace_kernel<true><<<(unsigned)blocks, threads, 0, stream>>>(p);
-  else
-    trace_kernel<false><<<(unsigned)blocks, threads, 0, stream>>>(p);
+  switch (out) {
+    case kOutRecord: trace_kernel<kOutRecord><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
+    case kOutSplat: trace_kernel<kOutSplat><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
+    default: trace_kernel<kOutFlux><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
+  }
   return cudaGetLastError();
 }
 

@@ -9,10 +9,12 @@ namespace qm {
 
 // tracer.cu built with FMA contraction (production) and without it
 // (every float operation rounded as the CPU oracle rounds it).
-cudaError_t launch_trace_fast(const TraceParams& p, bool record, cudaStream_t stream);
-cudaError_t launch_trace_exact(const TraceParams& p, bool record, cudaStream_t stream);
+// out: 0 flux into the receiver images, 1 per-ray outcome codes
+// (TraceParams::records), 2 bilinear deposit plus hit bits (TraceParams::hit_bits).
+cudaError_t launch_trace_fast(const TraceParams& p, int out, cudaStream_t stream);
+cudaError_t launch_trace_exact(const TraceParams& p, int out, cudaStream_t stream);
 // Production build limited to 48 registers (five 256-thread blocks per SM).
-cudaError_t launch_trace_fast4(const TraceParams& p, bool record, cudaStream_t stream);
+cudaError_t launch_trace_fast4(const TraceParams& p, int out, cudaStream_t stream);
 // Rays per warp chunk; TraceParams::facet_prefix counts chunks per task.
 int trace_chunk_rays_fast();
 int trace_chunk_rays_exact();

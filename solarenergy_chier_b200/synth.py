@@ -32,6 +32,28 @@ def sun_direction(azimuth_deg: float, elevation_deg: float) -> list[float]:
     return [-(math.cos(e) * math.sin(a)), -math.sin(e), -(math.cos(e) * math.cos(a))]
 
 
+def sun_positions(days: int = 12, hours: int = 8, latitude_deg: float = 37.0, min_elevation_deg: float = 15.0,
+                  max_elevation_deg: float = 80.0) -> np.ndarray:
+    """Sun directions (direction of travel) for `days` days spread over a year
+    (the 15th of each month for 12) x `hours` hours spread over the day
+    (hour angles -52.5..+52.5 degrees for 8), from the standard declination /
+    hour-angle formulas at `latitude_deg`, elevations clamped to
+    [min_elevation_deg, max_elevation_deg].  Shape (days * hours, 3), float32."""
+    lat = math.radians(latitude_deg)
+    out = []
+    for d in range(days):
+        day = 15 + round(365 * d / days)
+        decl = math.radians(23.45) * math.sin(2 * math.pi * (284 + day) / 365)
+        for k in range(hours):
+            h = math.radians(-52.5 + 105.0 * k / max(hours - 1, 1))
+            el = math.asin(math.sin(lat) * math.sin(decl) + math.cos(lat) * math.cos(decl) * math.cos(h))
+            el = min(max(el, math.radians(min_elevation_deg)), math.radians(max_elevation_deg))
+            az = math.atan2(-math.sin(h) * math.cos(decl),
+                            math.cos(lat) * math.sin(decl) - math.sin(lat) * math.cos(decl) * math.cos(h))
+            out.append(sun_direction(math.degrees(az), math.degrees(el)))
+    return np.array(out, np.float32)
+
+
 @dataclass
 class SceneFiles:
     scene: Path
