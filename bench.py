@@ -23,6 +23,8 @@ maximum over ranks.
 `batched` (--batched-lights, default 4 light indexes per sun) compares, over
 96 sun positions (12 days x 8 hours, elevations 15-80 deg), the plain path
 looped over the suns with one batch traced by a single CUDA-graph launch.
+`adjoint` (--adjoint-lights, default 32) times the differentiable forward and
+its adjoint (aim-point optimisation set-up) on the field.
 `reference_cuda` (--reference-cuda N) times the reference's own CUDA build
 on N heliostats spread over the field, and this tracer on the same ones.
 
@@ -58,6 +60,8 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--passes", type=int, default=32, help="light indexes per step")
+    p.add_argument("--adjoint-lights", type=int, default=32,
+                   help="light indexes of the adjoint/forward cost comparison (0 = skip)")
     p.add_argument("--batched-lights", type=int, default=4,
                    help="light indexes per sun of the 96-sun batched-vs-plain comparison (0 = skip)")
     p.add_argument("--impl", default="native", choices=["native", "reference"])
@@ -224,6 +228,58 @@ def batched_vs_plain(torch, scene, lights: int, stream):
             "plain_looped_mrays_s": rays / (plain_ms / 1e3) / 1e6, "batched_mrays_s": rays / (batched_ms / 1e3) / 1e6,
             "batched_graph_only_mrays_s": rays / (kernel_ms / 1e3) / 1e6,
             "speedup_batched_vs_plain": plain_ms / batched_ms, "plain_ms": plain_ms, "batched_ms": batched_ms}
+
+
+def adjoint_vs_forward(torch, scene, lights: int, stream):
+    """The differentiable pair on the field (aim-point optimisation set-up:
+    Gaussian splat sigma 2 px, L2 loss to a smooth seeded target with
+    peak/mean <= 2): device time of qmcrt_fwd (parameterised preparation,
+    bilinear-deposit trace, smoothing, loss) and of qmcrt_bwd (residual
+    smoothing, adjoint kernel), after two warm-up pairs, beside the plain
+    trace of the same rays."""
+    import numpy as np
+
+    import solarenergy_chier_b200 as q
+
+    d = q.Diff(scene, 2.0)
+    d.set_light_range(0, lights)
+    r = scene.receiver(0)
+    rows, cols = np.mgrid[0:r["height"], 0:r["width"]]
+    d.set_target(np.zeros((r["height"], r["width"]), np.float32))
+    d.forward(stream)
+    f0 = d.flux(0)
+    lit = f0 > 0.05 * f0.max()
+    rng = np.random.default_rng(7)
+    ph = rng.uniform(0, 2 * np.pi, 2)
+    bump = 1.0 + 0.5 * np.cos(2 * np.pi * cols / r["width"] * 3 + ph[0]) * np.cos(np.pi * rows / r["height"] + ph[1])
+    d.set_target((bump * lit * f0[lit].mean()).astype(np.float32))
+    H = scene.num_heliostats
+    d.set_params(rng.uniform(-0.5, 0.5, (H, 2)), rng.uniform(-5e-4, 5e-4, (H, 2)))
+    for _ in range(2):
+        d.forward(stream)
+        d.backward(stream)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    loss = d.forward(stream)
+    e[1].record(stream)
+    grad = d.backward(stream)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    fwd, bwd = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    scene.set_light_range(0, lights)
+    ids = list(range(H))
+    scene.trace(ids, stream)
+    torch.cuda.synchronize()
+    e[0].record(stream)
+    scene.trace(ids, stream)
+    e[1].record(stream)
+    torch.cuda.synchronize()
+    plain = e[0].elapsed_time(e[1])
+    d.close()
+    return {"lights": lights, "forward_ms": fwd, "adjoint_ms": bwd, "adjoint_over_forward": bwd / fwd,
+            "plain_trace_ms": plain, "forward_over_plain": fwd / plain, "loss": loss,
+            "grad_norm": float(np.linalg.norm(grad)), "sigma_px": 2.0}
 
 
 def cpu_baseline(files, seconds: float):
@@ -433,6 +489,8 @@ def main():
                 "roofline": roofline}
         if args.batched_lights > 0:
             line["batched"] = batched_vs_plain(torch, scene, args.batched_lights, stream)
+        if args.adjoint_lights > 0:
+            line["adjoint"] = adjoint_vs_forward(torch, scene, args.adjoint_lights, stream)
         if args.reference_cuda > 0:
             line["reference_cuda"] = reference_cuda(files, scene, args.reference_cuda)
         if not args.no_cpu_baseline:

@@ -197,6 +197,35 @@ int qmcrt_batch_autotune(qmcrt_batch* batch, void* stream, int* chosen_mode, flo
  * heliostat normals of one instance (either output may be NULL). */
 int qmcrt_batch_debug_geometry(qmcrt_batch* batch, int instance, int grid, float* vertices, float* normals);
 
+/* ---- differentiation ------------------------------------------------------
+ * No reference counterpart (the reference has no derivative of its tracer).
+ * A forward / adjoint pair over one scene at its current sun.  Parameters
+ * per heliostat h: aim offset (du, dv) in metres along the receiver's aim
+ * axes at the heliostat's aim point (cylinder: horizontal tangent and
+ * vertical; rectangle: its column and row edges) and normal offset (a, b)
+ * in radians about the u and v axes of the normal's frame.  The forward
+ * traces every heliostat with its parameters (sun shape, slope error,
+ * shadowing and blocking as the plain path), deposits each hit bilinearly at
+ * its pixel position, smooths with a normalised Gaussian of sigma_px pixels
+ * (flux F) and returns L = sum over pixels (F - target)^2 (FP64).  The adjoint
+ * returns dL/d(parameters), 4 doubles per heliostat (du, dv, a, b), from a
+ * hand-written forward-mode kernel along each hit ray, with shadowing and
+ * blocking indicators detached and the receiver's edges treated by band
+ * estimates of their boundary terms; hit records of the forward are kept
+ * (1 bit per ray).  Common random numbers: the scene's pools and facet
+ * offsets are reused by every forward. */
+typedef struct qmcrt_diff qmcrt_diff;
+int qmcrt_diff_create(qmcrt_scene* scene, float sigma_px, qmcrt_diff** out);
+void qmcrt_diff_free(qmcrt_diff* diff);
+/* aim_offsets, normal_offsets: 2 floats per heliostat each (NULL = zeros). */
+int qmcrt_diff_set_params(qmcrt_diff* diff, const float* aim_offsets, const float* normal_offsets);
+int qmcrt_diff_set_target(qmcrt_diff* diff, int receiver, const float* target);
+int qmcrt_diff_set_light_range(qmcrt_diff* diff, int begin, int end);
+int qmcrt_fwd(qmcrt_diff* diff, double* loss, void* stream);
+int qmcrt_bwd(qmcrt_diff* diff, double* grad, void* stream);
+/* The smoothed flux F of the last forward. */
+int qmcrt_diff_flux(qmcrt_diff* diff, int receiver, float* out, int* width, int* height);
+
 /* ---- smoothing and output ------------------------------------------------
  * Replaces ImageSmoother::image_smooth (Tool/Smoother/ImageSmoother.cu:68-113):
  * in-place trimmed mean of a device image.  0 <= trim_ratio < 0.5. */

@@ -8,6 +8,7 @@ from ._lib import LIB_PATH, QmcrtError, load  # noqa: F401
 from .scene import (  # noqa: F401
     SUNSHAPE_BUIE,
     Batch,
+    Diff,
     SUNSHAPE_PILLBOX,
     ImageSaver,
     ImageSmoother,
@@ -21,7 +22,7 @@ from .scene import (  # noqa: F401
 )
 
 __all__ = [
-    "Scene", "Batch", "QuasiMonteCarloRayTracer", "ImageSmoother", "ImageSaver", "RayTracingPipeline",
+    "Scene", "Batch", "Diff", "QuasiMonteCarloRayTracer", "ImageSmoother", "ImageSaver", "RayTracingPipeline",
     "SUNSHAPE_BUIE", "SUNSHAPE_PILLBOX", "QmcrtError", "load", "LIB_PATH", "save_text", "smooth_device",
     "pipeline_run", "executable",
 ]

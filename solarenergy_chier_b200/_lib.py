@@ -91,6 +91,14 @@ PROTOTYPES = {
     "qmcrt_batch_power_fp64": (_i, [_vp, _i, _pd, _pd]),
     "qmcrt_batch_autotune": (_i, [_vp, _vp, _pi, _pf]),
     "qmcrt_batch_debug_geometry": (_i, [_vp, _i, _i, _pf, _pf]),
+    "qmcrt_diff_create": (_i, [_vp, _f, ctypes.POINTER(_vp)]),
+    "qmcrt_diff_free": (None, [_vp]),
+    "qmcrt_diff_set_params": (_i, [_vp, _pf, _pf]),
+    "qmcrt_diff_set_target": (_i, [_vp, _i, _pf]),
+    "qmcrt_diff_set_light_range": (_i, [_vp, _i, _i]),
+    "qmcrt_fwd": (_i, [_vp, _pd, _vp]),
+    "qmcrt_bwd": (_i, [_vp, _pd, _vp]),
+    "qmcrt_diff_flux": (_i, [_vp, _i, _pf, _pi, _pi]),
 }
 
 _lib = None

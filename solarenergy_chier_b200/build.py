@@ -34,7 +34,7 @@ HOST_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-Wall", "-Wno-
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-ffp-contract=off"] + ARCH
 
-HOST_SOURCES = ["scene.cpp", "buie_table.cpp", "capi.cpp", "batch.cpp", "pipeline.cpp"]
+HOST_SOURCES = ["scene.cpp", "buie_table.cpp", "capi.cpp", "batch.cpp", "diff.cpp", "pipeline.cpp"]
 CUDA_UNITS = [
     ("tracer.cu", "tracer_fast.o", ["-DQM_TRACE_VARIANT=fast", "-DQM_TRACE_MIN_BLOCKS=4"]),
     ("tracer.cu", "tracer_fast4.o", ["-DQM_TRACE_VARIANT=fast4", "-DQM_TRACE_MIN_BLOCKS=5"]),
@@ -42,6 +42,7 @@ CUDA_UNITS = [
     ("pools.cu", "pools.o", []),
     # per-sun preparation: no FMA contraction, so it matches the host geometry bit for bit
     ("prep.cu", "prep.o", ["-fmad=false"]),
+    ("diff.cu", "diff_kernels.o", []),
     ("smooth.cu", "smooth.o", []),
     ("microbench.cu", "microbench.o", []),
     ("smooth_static.cu", "smooth_static.o", []),

@@ -112,6 +112,7 @@ cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out) {
   p.light_end = b->light_end;
   p.power = b->d_power.as<double>();
   p.diag = b->d_diag.as<unsigned long long>();
+  p.hit_bits = b->hit_bits;
   switch (b->mode) {
     case 1: return qm::launch_trace_exact(p, out, st);
     case 2: return qm::launch_trace_fast4(p, out, st);

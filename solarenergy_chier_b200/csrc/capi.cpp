@@ -131,8 +131,17 @@ void build_device_scene(qmcrt_scene* s) {
   s->grids.clear();
   for (auto& g : m.grids) {
     auto gb = std::make_unique<GridBufs>();
-    upload(gb->hindex, g.cell_hindex);
-    upload(gb->hmatch, g.cell_hmatch);
+    // Cell lists in traversal form: a [begin, end) pair per cell and, per
+    // entry, the heliostat with its sub-heliostat range inline.
+    std::vector<int2> ranges(g.cell_hindex.size() > 0 ? g.cell_hindex.size() - 1 : 0);
+    for (size_t c = 0; c < ranges.size(); ++c) ranges[c] = make_int2(g.cell_hindex[c], g.cell_hindex[c + 1]);
+    std::vector<int4> entries(g.cell_hmatch.size());
+    for (size_t k = 0; k < entries.size(); ++k) {
+      const qm::HeliostatModel& h = m.heliostats[g.start_heliostat + g.cell_hmatch[k]];
+      entries[k] = make_int4(g.cell_hmatch[k], h.sub_begin, h.num_sub, 0);
+    }
+    upload(gb->ranges, ranges);
+    upload(gb->entries, entries);
     std::vector<float4> bound, subv;
     std::vector<int4> hsub;
     grid_sun_data(m, g, bound, hsub, subv);
@@ -144,8 +153,8 @@ void build_device_scene(qmcrt_scene* s) {
     dg.interval = g.interval;
     dg.cells = g.cells;
     dg.max_steps = g.cells.x + g.cells.y + g.cells.z + 2;
-    dg.hindex = gb->hindex.as<int>();
-    dg.hmatch = gb->hmatch.as<int>();
+    dg.cell_range = gb->ranges.as<int2>();
+    dg.entries = gb->entries.as<int4>();
     dg.bound = gb->bound.as<float4>();
     dg.hsub = gb->hsub.as<int4>();
     dg.subv = gb->subv.as<float4>();

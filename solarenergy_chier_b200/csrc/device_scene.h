@@ -14,8 +14,8 @@ struct DevGrid {
   float3 interval;
   int3 cells;
   int max_steps;        // DDA step bound: cells.x + cells.y + cells.z + 2
-  const int* hindex;    // heliostat-level CSR offsets, cells + 1 entries
-  const int* hmatch;    // grid-local heliostat ids per cell
+  const int2* cell_range;  // [begin, end) of each cell's entries
+  const int4* entries;     // per cell entry: grid-local heliostat id, first sub-heliostat, count, 0
   const float4* bound;  // 5 float4 per grid-local heliostat: (centre, window margin), (axis_k, half extent_k)
                         // for k = lattice x, normal, lattice z, then (x0, 1/px, z0, 1/pz)
   const int4* hsub;     // (first sub-heliostat id, count, lattice rows, lattice columns) per grid-local heliostat
@@ -26,6 +26,7 @@ struct DevReceiver {
   int type;             // 0 rectangle, 1 cylinder
   int2 resolution;      // x = columns, y = rows
   float* image;         // resolution.x * resolution.y floats, row-major by row
+  double* deposit;      // bilinear-deposit launches: FP64 accumulator of the same shape (else unused)
   float3 a, ab, ac;     // rectangle: vertex 0, v1 - v0, v3 - v0
   float3 pos, size;     // cylinder: centre, (radius, height, -)
 };

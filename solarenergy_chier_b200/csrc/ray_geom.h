@@ -46,16 +46,16 @@ __device__ __forceinline__ bool receiver_hit(const DevReceiver& r, float3 o, flo
   return cylinder_hit(r, o, d, t, u, v);
 }
 
-// Micro-facet centre and normal (rectangle_heliostat::map_microhelio_center_and_normal,
+// Micro-facet centres and normals (rectangle_heliostat::map_microhelio_center_and_normal,
 // Scene/DataStructure/Heliostat/RectangleHelio.cu:54-80; focusFlatRectangle_heliostat
 // kernels, FocusFlatRectangleHelio.cu:12-64), evaluated per facet instead of
-// materialised; explicitly rounded (once per facet, off the hot path).
-__device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& origin, float3& normal) {
-  Frame hf;
-  hf.u = T.fu;
-  hf.n = T.fn;
-  hf.v = T.fv;
-  hf.identity = T.frame_identity != 0;
+// materialised; explicitly rounded.
+//
+// Micro-facet f in its heliostat's local frame: its centre (the point the
+// heliostat frame turns into world space) and, for focus-flat heliostats,
+// the local normal of its sub-heliostat (flat facets share the heliostat
+// normal).  Returns true for focus-flat.
+__device__ __forceinline__ bool facet_local(const DevTask& T, int f, float3& local, float3& local_normal) {
   const int per_row = T.row_col.y * T.sub_row_col.y;
   int row = f / per_row;
   int col = f % per_row;
@@ -63,26 +63,37 @@ __device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& 
   if (T.type == 0) {
     int brow = row / T.sub_row_col.x;
     int bcol = col / T.sub_row_col.y;
-    float3 c;
-    c.x = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)col, px), qm_rn_mul((float)bcol, T.gap.x)), px / 2),
-                    T.size.x / 2);
-    c.y = T.size.y / 2;
-    c.z = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)row, px), qm_rn_mul((float)brow, T.gap.y)), px / 2),
-                    T.size.z / 2);
-    origin = qs::add(qs::to_world(hf, c), T.pos);
-    normal = T.normal;
-  } else {
-    int block = (row / T.sub_row_col.x) * T.row_col.y + col / T.sub_row_col.y;
-    float3 ln = T.local_normals[block];
-    float3 lc = T.local_centers[block];
-    row %= T.sub_row_col.x;
-    col %= T.sub_row_col.y;
-    float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)col, 0.5f), px), T.sub_length.y / 2), 0.0f,
-                            qm_rn_sub(qm_rn_mul(qm_rn_add((float)row, 0.5f), px), T.sub_length.x / 2));
-    lp = qs::add(qs::rotate_to(lp, ln, true), lc);
-    normal = qs::to_world(hf, ln);
-    origin = qs::add(qs::to_world(hf, lp), T.pos);
+    local.x = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)col, px), qm_rn_mul((float)bcol, T.gap.x)), px / 2),
+                        T.size.x / 2);
+    local.y = T.size.y / 2;
+    local.z = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)row, px), qm_rn_mul((float)brow, T.gap.y)), px / 2),
+                        T.size.z / 2);
+    local_normal = make_float3(0.f, 1.f, 0.f);
+    return false;
   }
+  int block = (row / T.sub_row_col.x) * T.row_col.y + col / T.sub_row_col.y;
+  const float3 ln = T.local_normals[block];
+  const float3 lc = T.local_centers[block];
+  row %= T.sub_row_col.x;
+  col %= T.sub_row_col.y;
+  float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)col, 0.5f), px), T.sub_length.y / 2), 0.0f,
+                          qm_rn_sub(qm_rn_mul(qm_rn_add((float)row, 0.5f), px), T.sub_length.x / 2));
+  local = qs::add(qs::rotate_to(lp, ln, true), lc);
+  local_normal = ln;
+  return true;
+}
+
+// Micro-facet f in world space.
+__device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& origin, float3& normal) {
+  Frame hf;
+  hf.u = T.fu;
+  hf.n = T.fn;
+  hf.v = T.fv;
+  hf.identity = T.frame_identity != 0;
+  float3 local, ln;
+  const bool focus_flat = facet_local(T, f, local, ln);
+  normal = focus_flat ? qs::to_world(hf, ln) : T.normal;
+  origin = qs::add(qs::to_world(hf, local), T.pos);
 }
 
 __device__ __forceinline__ int find_task(const long long* prefix, int n, long long w) {

@@ -84,7 +84,7 @@ void upload(DBuf& b, const std::vector<T>& v) {
 }
 
 struct GridBufs {
-  DBuf hindex, hmatch, bound, hsub, subv;
+  DBuf ranges, entries, bound, hsub, subv;
 };
 
 class DeviceGuard {

@@ -86,12 +86,13 @@ __device__ __forceinline__ int band(float x, float inv_pitch, int n) {
 }
 
 // The ray against one heliostat's traversal record (5 float4, built by the
-// host): false if it misses the padded box, else the window of lattice rows
-// [r0, r1] and columns [c0, c1] holding every sub-heliostat it can hit --
-// the lattice bands met by the ray's own extent inside the box, widened by
-// the record's window margin.
-__device__ __forceinline__ bool box_window(const float4* b, int rows, int cols, float3 o, float3 d, int& r0,
-                                           int& r1, int& c0, int& c1) {
+// host or the preparation kernel): false if it misses the padded box, else
+// the window of lattice rows [r0, r1] and columns [c0, c1] holding every
+// sub-heliostat it can hit -- the lattice bands met by the ray's own extent
+// inside the box, widened by the record's window margin.  The lattice shape
+// (hs: first, count, rows, columns) is read only when the box is entered.
+__device__ __forceinline__ bool box_window(const float4* b, const int4* hs, float3 o, float3 d, int& r0, int& r1,
+                                           int& c0, int& c1, int& cols) {
   const float4 c = __ldg(b);
   const float3 r = make_float3(o.x - c.x, o.y - c.y, o.z - c.z);
   const float4 an = __ldg(b + 2);
@@ -109,6 +110,9 @@ __device__ __forceinline__ bool box_window(const float4* b, int rows, int cols, 
   slab(olz, dlz, az.w, tn, tf);
   if (!(tn <= tf && tf >= -1.0f)) return false;
   tn = fmaxf(tn, -1.0f);
+  const int4 lattice = __ldg(hs);  // first, count, rows, columns
+  const int rows = lattice.z;
+  cols = lattice.w;
   const float4 lat = __ldg(b + 4);  // x0, 1/px, z0, 1/pz
   const float xa = olx + tn * dlx, xb = olx + tf * dlx;
   const float za = olz + tn * dlz, zb = olz + tf * dlz;
@@ -134,22 +138,22 @@ __device__ __forceinline__ bool sub_hit(const float4* sv, float3 o, float3 d) {
 // just the sub-heliostats inside the ray's window gives the same answer.
 __device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, float3 o, float3 d, int& seen0,
                                          int& seen1) {
-  int b = __ldg(g.hindex + cell), e = __ldg(g.hindex + cell + 1);
-  for (int k = b; k < e; ++k) {
-    int h = __ldg(g.hmatch + k);
+  const int2 range = __ldg(g.cell_range + cell);
+  for (int k = range.x; k < range.y; ++k) {
+    const int4 en = __ldg(g.entries + k);  // heliostat, first sub-heliostat, count
+    const int h = en.x;
     if (h == own || h == seen0 || h == seen1) continue;
-    const int4 hs = __ldg(g.hsub + h);  // first sub-heliostat, count, lattice rows, lattice columns
     seen1 = seen0;
     seen0 = h;
-    if (hs.y == 1) {
-      if (sub_hit(g.subv + 3 * hs.x, o, d)) return true;
+    if (en.z == 1) {
+      if (sub_hit(g.subv + 3 * en.y, o, d)) return true;
       continue;
     }
-    int r0, r1, c0, c1;
-    if (!box_window(g.bound + 5 * h, hs.z, hs.w, o, d, r0, r1, c0, c1)) continue;
+    int r0, r1, c0, c1, cols;
+    if (!box_window(g.bound + 5 * h, g.hsub + h, o, d, r0, r1, c0, c1, cols)) continue;
     for (int rr = r0; rr <= r1; ++rr)
       for (int cc = c0; cc <= c1; ++cc)
-        if (sub_hit(g.subv + 3 * (hs.x + rr * hs.w + cc), o, d)) return true;
+        if (sub_hit(g.subv + 3 * (en.y + rr * cols + cc), o, d)) return true;
   }
   return false;
 }
@@ -318,6 +322,8 @@ enum TraceOut { kOutFlux = 0, kOutRecord = 1, kOutSplat = 2 };
 // Bilinear deposit of energy e at continuous pixel position (X, Y) (pixel c
 // spans [c, c+1), centres at c + 0.5): columns wrap around for a cylinder
 // (its columns are angles), everything else outside the image is dropped.
+// Accumulated in FP64, so the deposit (and the loss computed from it) does
+// not depend on the order of the atomic additions.
 __device__ __forceinline__ void splat_bilinear(const DevReceiver& R, float X, float Y, float e) {
   const float x = X - 0.5f, y = Y - 0.5f;
   const float x0 = floorf(x), y0 = floorf(y);
@@ -331,7 +337,7 @@ __device__ __forceinline__ void splat_bilinear(const DevReceiver& R, float X, fl
     const float wgt = ((k & 1) ? fx : 1.0f - fx) * ((k >> 1) ? fy : 1.0f - fy);
     if (wrap) c = c < 0 ? c + w : (c >= w ? c - w : c);
     if (c < 0 || c >= w || r < 0 || r >= h) continue;
-    atomicAdd(R.image + r * w + c, e * wgt);
+    atomicAdd(R.deposit + r * w + c, (double)(e * wgt));
   }
 }
 

@@ -333,6 +333,68 @@ class Batch:
         return per, total.value
 
 
+class Diff:
+    """Differentiable forward / adjoint over one scene (qmcrt_diff_*, qmcrt_fwd, qmcrt_bwd).
+
+    Parameters per heliostat: aim offset (du, dv) in metres and normal offset
+    (a, b) in radians; `forward()` returns the loss against the target flux,
+    `backward()` its gradient, shape (num_heliostats, 4)."""
+
+    def __init__(self, scene: Scene, sigma_px: float = 2.0):
+        self._lib = load()
+        self._scene = scene  # the scene must outlive the pair
+        h = ctypes.c_void_p()
+        check(self._lib.qmcrt_diff_create(scene.handle, float(sigma_px), ctypes.byref(h)))
+        self._h = h
+        self.num_heliostats = scene.num_heliostats
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.qmcrt_diff_free(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, aim=None, normal=None) -> None:
+        def arr(x):
+            if x is None:
+                return None, None
+            a = np.ascontiguousarray(np.asarray(x, np.float32).reshape(self.num_heliostats, 2))
+            return a, _ptr(a, ctypes.c_float)
+
+        a, pa = arr(aim)
+        n, pn = arr(normal)
+        check(self._lib.qmcrt_diff_set_params(self._h, pa, pn))
+
+    def set_target(self, target: np.ndarray, receiver: int = 0) -> None:
+        t = np.ascontiguousarray(np.asarray(target, np.float32))
+        check(self._lib.qmcrt_diff_set_target(self._h, receiver, _ptr(t, ctypes.c_float)))
+
+    def set_light_range(self, begin: int, end: int) -> None:
+        check(self._lib.qmcrt_diff_set_light_range(self._h, begin, end))
+
+    def forward(self, stream=None) -> float:
+        loss = ctypes.c_double()
+        check(self._lib.qmcrt_fwd(self._h, ctypes.byref(loss), _stream_handle(stream)))
+        return loss.value
+
+    def backward(self, stream=None) -> np.ndarray:
+        g = np.zeros((self.num_heliostats, 4), np.float64)
+        check(self._lib.qmcrt_bwd(self._h, _ptr(g, ctypes.c_double), _stream_handle(stream)))
+        return g
+
+    def flux(self, receiver: int = 0) -> np.ndarray:
+        w, h = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.qmcrt_diff_flux(self._h, receiver, None, ctypes.byref(w), ctypes.byref(h)))
+        out = np.zeros((h.value, w.value), np.float32)
+        check(self._lib.qmcrt_diff_flux(self._h, receiver, _ptr(out, ctypes.c_float), ctypes.byref(w), ctypes.byref(h)))
+        return out
+
+
 def smooth_device(device_ptr: int, width: int, height: int, radius: int, ratio: float, stream=None) -> None:
     """In-place trimmed mean of a device image (qmcrt_smooth)."""
     check(load().qmcrt_smooth(ctypes.c_void_p(device_ptr), width, height, radius, float(ratio),
