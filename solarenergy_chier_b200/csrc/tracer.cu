@@ -42,9 +42,18 @@ namespace qm {
 namespace {
 
 // rectGridDDA::absDivide / calTMax / equal / less (rectGridDDA.cuh:15-32).
+// The production builds (QM_TRACE_FAST_DIVIDE) divide with the approximate
+// reciprocal (within 2 ulp): the quotients only set the order in which the
+// walk crosses cell boundaries, which they change only for boundaries within
+// a few ulp of a 1e-5 tie.  The exact build divides correctly rounded, as the
+// reference does.
 __device__ __forceinline__ float abs_divide(float den, float num) {
   if (qm_below_eps(num) && qm_above_neg_eps(num)) return (float)INT_MAX;
+#if defined(QM_TRACE_FAST_DIVIDE)
+  return fabsf(__fdividef(den, num));
+#else
   return fabsf(den / num);
+#endif
 }
 __device__ __forceinline__ float cal_tmax(float dir, float interval, int index, float pos) {
   return fabsf(float(index + (dir >= 0)) * interval - pos);
