@@ -151,6 +151,12 @@ int qmcrt_power_clear(qmcrt_scene* scene);
  * [1] grid walks stopped by the step bound, [2..3] reserved. */
 int qmcrt_diagnostics(qmcrt_scene* scene, unsigned long long* out4);
 
+/* Debug: per heliostat, 1 when the tracer skips its shadow walks for the
+ * current sun and pool because no other heliostat can shadow any of its rays
+ * (a conservative capsule test around the sun-shape cone; no reference
+ * counterpart -- the reference walks every ray). */
+int qmcrt_debug_shadow_free(qmcrt_scene* scene, int* flags);
+
 /* Per-ray outcome for facets [facet_begin, facet_end) x lights [light_begin,
  * light_end) of one heliostat, row-major by facet: pixel index for a
  * receiver hit, -1 shadowed, -2 blocked, -3 missed the receiver.  Traces into

@@ -57,7 +57,15 @@ void batch_prepare(qmcrt_batch* b, cudaStream_t st) {
   for (size_t k = 0; k < b->inst.size(); ++k) {
     const auto& I = b->inst[k];
     const int H = (int)I.scene->model.heliostats.size();
-    for (int h = 0; h < H; ++h) b->items[I.task_base + h].sun_dir = I.sun;
+    float3 axis;
+    float tan_world;
+    sun_cone(I.sun, I.scene->sun_shape_tan, axis, tan_world);
+    for (int h = 0; h < H; ++h) {
+      qm::PrepItem& it = b->items[I.task_base + h];
+      it.sun_dir = I.sun;
+      it.shadow_axis = axis;
+      it.shadow_tan = tan_world;
+    }
   }
   cuda_check(cudaMemcpyAsync(b->d_tasks.p, b->tasks.data(), b->tasks.size() * sizeof(qm::DevTask),
                              cudaMemcpyHostToDevice, st),
@@ -67,6 +75,9 @@ void batch_prepare(qmcrt_batch* b, cudaStream_t st) {
              "prep upload");
   cuda_check(qm::launch_prep(b->d_items.as<qm::PrepItem>(), (int)b->items.size(), b->d_tasks.as<qm::DevTask>(), st),
              "prep kernel");
+  cuda_check(qm::launch_shadow_flags(b->d_items.as<qm::PrepItem>(), (int)b->items.size(), b->d_tasks.as<qm::DevTask>(),
+                                     b->d_grids.as<qm::DevGrid>(), st),
+             "shadow flags");
   std::vector<qm::PoolRotation> rot(b->inst.size());
   int max_out = 0;
   for (size_t k = 0; k < b->inst.size(); ++k) {

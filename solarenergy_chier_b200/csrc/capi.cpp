@@ -1,6 +1,7 @@
 // C ABI (include/qmcrt.h) over the host scene model and the sm_100a kernels.
 #include "qmcrt.h"
 #include "helio_geom.h"
+#include "shadow.h"
 
 #include <cuda_runtime.h>
 
@@ -142,9 +143,12 @@ void build_device_scene(qmcrt_scene* s) {
     }
     upload(gb->ranges, ranges);
     upload(gb->entries, entries);
+    gb->h_ranges = ranges;
+    gb->h_entries = entries;
     std::vector<float4> bound, subv;
     std::vector<int4> hsub;
     grid_sun_data(m, g, bound, hsub, subv);
+    gb->h_bound = bound;
     upload(gb->bound, bound);
     upload(gb->hsub, hsub);
     upload(gb->subv, subv);
@@ -236,14 +240,63 @@ void generate_offsets(qmcrt_scene* s, unsigned seed) {
   cuda_check(cudaDeviceSynchronize(), "offsets kernel");
 }
 
+// Sun axis and tangent of the largest sun-shape angle in world space, for
+// the shadow-free test, from the tangent `tan_local` of the local pool (the
+// sun frame maps the local y axis to -sun_dir, which may not be unit length;
+// an identity frame leaves samples as they are).
+void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world) {
+  const qm::Frame f = qm::make_frame(qm::neg(sun_dir), false);
+  if (f.identity) {
+    axis = make_float3(0.f, 1.f, 0.f);
+    tan_world = tan_local;
+    return;
+  }
+  axis = qm::neg(sun_dir);
+  const double len = std::sqrt((double)sun_dir.x * sun_dir.x + (double)sun_dir.y * sun_dir.y +
+                               (double)sun_dir.z * sun_dir.z);
+  tan_world = tan_local < 0.0f ? -1.0f : (float)(tan_local / len);
+}
+
+// Shadow-free flags of every heliostat's template for the current sun and
+// pool (qm::shadow_free, csrc/shadow.h).
+void update_shadow_flags(qmcrt_scene* s) {
+  std::vector<float4> pool(s->pool_size);
+  cuda_check(cudaMemcpy(pool.data(), s->d_samples.p, pool.size() * sizeof(float4), cudaMemcpyDeviceToHost),
+             "pool readback");
+  double tmax = 0.0;
+  for (const float4& q : pool) {
+    if (!(q.y > 0.0f)) {
+      tmax = -1.0;
+      break;
+    }
+    tmax = std::max(tmax, std::sqrt((double)q.x * q.x + (double)q.z * q.z) / q.y);
+  }
+  s->sun_shape_tan = (float)tmax;
+  float3 axis;
+  float tan_world;
+  sun_cone(s->model.config.sun_dir, s->sun_shape_tan, axis, tan_world);
+  const qm::SceneModel& m = s->model;
+  for (size_t i = 0; i < m.heliostats.size(); ++i) {
+    const int g = m.heliostats[i].grid;
+    const qm::GridModel& gm = m.grids[g];
+    const GridBufs& gb = *s->grid_bufs[g];
+    qm::ShadowGrid view{gm.pos, gm.interval, gm.cells, gb.h_bound.data(), gb.h_ranges.data(), gb.h_entries.data()};
+    s->templates[i].shadow_free =
+        tan_world >= 0.0f && qm::shadow_free(view, (int)i - gm.start_heliostat, axis, tan_world) ? 1 : 0;
+  }
+  s->cache_valid = false;
+}
+
 // The tracer's copies of the pools (world-space samples, P + L entries);
-// redone after every change of the pools or of the sun.
+// redone after every change of the pools or of the sun, with the
+// shadow-free flags that depend on both.
 void rotate_pool(qmcrt_scene* s) {
   const int n_out = s->pool_size + s->model.config.num_per_sunshape_group;
   cuda_check(qm::launch_trace_pools(s->d_samples.as<float4>(), s->d_perturb.as<float4>(), s->pool_size, n_out, s->sun,
                                     s->d_trace_samples.as<float4>(), s->d_trace_perturb.as<float4>(), 0),
              "pool rotation");
   cuda_check(cudaDeviceSynchronize(), "pool rotation");
+  update_shadow_flags(s);
 }
 
 void generate_pool(qmcrt_scene* s, unsigned seed, int sunshape, float half_angle) {
@@ -566,6 +619,7 @@ int qmcrt_scene_set_sun(qmcrt_scene* s, const float* sun_dir) {
       std::vector<float4> bound, subv;
       std::vector<int4> hsub;
       grid_sun_data(s->model, s->model.grids[g], bound, hsub, subv);
+      s->grid_bufs[g]->h_bound = bound;
       upload(s->grid_bufs[g]->bound, bound);
       upload(s->grid_bufs[g]->hsub, hsub);
       upload(s->grid_bufs[g]->subv, subv);
@@ -769,6 +823,14 @@ int qmcrt_diagnostics(qmcrt_scene* s, unsigned long long* out4) {
     cuda_check(cudaDeviceSynchronize(), "synchronise");
     cuda_check(cudaMemcpy(out4, s->d_diag.p, qm::kDiagSlots * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
                "readback");
+  });
+}
+
+int qmcrt_debug_shadow_free(qmcrt_scene* s, int* flags) {
+  return guarded([&] {
+    checked(s);
+    if (!flags) invalid("output is NULL");
+    for (size_t i = 0; i < s->templates.size(); ++i) flags[i] = s->templates[i].shadow_free;
   });
 }
 

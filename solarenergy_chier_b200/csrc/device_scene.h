@@ -57,6 +57,7 @@ struct DevTask {
   const float4* samples;        // sun-shape pool already turned into world space by this task's sun
   const float4* perturbations;  // slope-error pool (local frame of the facet normal)
   int pool_size;                // P = groups x lights per group
+  int shadow_free;              // no ray of this heliostat can be shadowed: shadow walks skipped
 };
 
 struct SunFrame {

@@ -13,6 +13,7 @@
 #include "prep.h"
 
 #include "helio_geom.h"
+#include "shadow.h"
 
 namespace qm {
 namespace {
@@ -61,6 +62,16 @@ __global__ void prep_kernel(const PrepItem* items, int n, DevTask* tasks) {
   *it.hsub = make_int4(it.sub_first, it.num_sub, rc.x, rc.y);
 }
 
+__global__ void shadow_kernel(const PrepItem* items, int n, DevTask* tasks, const DevGrid* grids) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const PrepItem it = items[i];
+  DevTask& T = tasks[it.task];
+  const DevGrid& G = grids[T.grid];
+  const ShadowGrid view{G.pos, G.interval, G.cells, G.bound, G.cell_range, G.entries};
+  T.shadow_free = it.shadow_tan >= 0.0f && shadow_free(view, T.own, it.shadow_axis, it.shadow_tan) ? 1 : 0;
+}
+
 // Pool of instance blockIdx.y turned by that instance's sun frame.
 __global__ void rotate_pools_kernel(const PoolRotation* jobs) {
   const PoolRotation J = jobs[blockIdx.y];
@@ -84,6 +95,13 @@ __global__ void rotate_pools_kernel(const PoolRotation* jobs) {
 cudaError_t launch_prep(const PrepItem* items, int n, DevTask* tasks, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   prep_kernel<<<(n + 127) / 128, 128, 0, stream>>>(items, n, tasks);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shadow_flags(const PrepItem* items, int n, DevTask* tasks, const DevGrid* grids,
+                                cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  shadow_kernel<<<(n + 127) / 128, 128, 0, stream>>>(items, n, tasks, grids);
   return cudaGetLastError();
 }
 

@@ -22,6 +22,10 @@ struct PrepItem {
   // normal_offset (radians) about the u and v axes of its own frame.
   float2 aim_offset, normal_offset;
   float3 aim_u, aim_v;
+  // Shadow-free test (qm::shadow_free): sun axis and world-space tangent of
+  // the largest sun-shape angle (< 0: unbounded, never shadow-free).
+  float3 shadow_axis;
+  float shadow_tan;
   float3* verts;    // out: 3 float3 (B, A, C) per sub-heliostat
   float4* subv;     // out: 3 float4 per sub-heliostat (A, B - A, C - A)
   float4* bound;    // out: 5 float4 traversal record
@@ -36,6 +40,10 @@ struct PoolRotation {
 };
 
 cudaError_t launch_prep(const PrepItem* items, int n, DevTask* tasks, cudaStream_t stream);
+// Shadow-free flags of the prepared tasks; grids: the tasks' grids with their
+// prepared traversal records.  Run after launch_prep.
+cudaError_t launch_shadow_flags(const PrepItem* items, int n, DevTask* tasks, const DevGrid* grids,
+                                cudaStream_t stream);
 // max_out: the largest n_out of the jobs.
 cudaError_t launch_rotate_pools(const PoolRotation* jobs, int n_jobs, int max_out, cudaStream_t stream);
 

@@ -85,6 +85,10 @@ void upload(DBuf& b, const std::vector<T>& v) {
 
 struct GridBufs {
   DBuf ranges, entries, bound, hsub, subv;
+  // host copies for the shadow-free test
+  std::vector<float4> h_bound;
+  std::vector<int2> h_ranges;
+  std::vector<int4> h_entries;
 };
 
 class DeviceGuard {
@@ -120,6 +124,7 @@ struct qmcrt_scene {
   qrt::DBuf d_offsets;
   std::vector<long long> offset_base;
   qrt::DBuf d_samples, d_perturb;
+  float sun_shape_tan = -1.0f;  // tan of the largest sun-shape angle of the local pool (< 0: unbounded)
   qrt::DBuf d_trace_samples;  // tracer copy: d_samples in world space, P + L entries (entry i = i % P)
   qrt::DBuf d_trace_perturb;  // tracer copy of d_perturb, P + L entries
   qrt::DBuf d_offset_seg;     // heliostats + 1 starts of the per-heliostat offset segments
@@ -174,6 +179,9 @@ namespace qrt {
 void grid_sun_data(const qm::SceneModel& m, const qm::GridModel& g, std::vector<float4>& bound,
                    std::vector<int4>& hsub, std::vector<float4>& subv);
 qmcrt_scene* checked(qmcrt_scene* s);
+// Sun axis and world-space tangent of the largest sun-shape angle for the
+// shadow-free test (tan_local < 0: unbounded, tan_world < 0).
+void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world);
 cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st);
 int trace_chunk_rays();
 constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;

@@ -1,0 +1,131 @@
+// Per-heliostat shadow-free test, shared by the host (plain scenes) and the
+// device (batch preparation).
+//
+// The reference walks every ray toward the sun through the grid
+// (rectGridDDA::collision, rectGridDDA.cu:31-119) and tests the
+// sub-heliostats of every heliostat listed in the cells it visits.  A ray of
+// heliostat i starts on one of its facets -- inside its padded box, so
+// within r_i (the box's half diagonal) of the box centre c -- and travels
+// along a sun-shape direction within angle theta of the sun axis a.  Every
+// point q of such a ray, at axis parameter s = (q - c).a >= -r_i, lies
+// within r_i + (s + r_i) tan(theta) / cos(theta) of the axis line.  So if
+// no other heliostat j listed in a cell the rays can visit has its padded
+// box within that distance of the axis -- tested as the axis ray against
+// box j widened by the distance reached at j's far side, plus a margin far
+// above float rounding -- no ray of heliostat i can be shadowed, and its
+// shadow walks are skipped with the same result.  The cells a ray can
+// visit lie in the grid and inside the same distance of the axis, so they
+// are covered by the bounding box of that capsule up to where it leaves the
+// grid.  The test is conservative: "false" only means the walks are done.
+#pragma once
+
+#include "vecmath.h"
+
+namespace qm {
+
+struct ShadowGrid {
+  float3 pos, interval;
+  int3 cells;
+  const float4* bound;    // 5 float4 per grid-local heliostat (centre, then axes with half extents)
+  const int2* ranges;     // [begin, end) of each cell's entries
+  const int4* entries;    // grid-local heliostat id first
+};
+
+// Ray (o, a) against the box of record b widened by w on every axis: true
+// when they meet at an axis parameter >= s_min.
+QM_HD bool shadow_box_meets(const float4* b, float w, float3 o, float3 a, float s_min) {
+  const float3 r = make_float3(o.x - b[0].x, o.y - b[0].y, o.z - b[0].z);
+  float tn = -3.0e38f, tf = 3.0e38f;
+  for (int k = 1; k <= 3; ++k) {
+    const float4 ax = b[k];
+    const float ol = r.x * ax.x + r.y * ax.y + r.z * ax.z;
+    const float dl = a.x * ax.x + a.y * ax.y + a.z * ax.z;
+    const float half = ax.w + w;
+    if (fabsf(dl) < 1e-12f) {
+      if (fabsf(ol) > half) return false;
+      continue;
+    }
+    const float t0 = (-half - ol) / dl, t1 = (half - ol) / dl;
+    tn = fmaxf(tn, fminf(t0, t1));
+    tf = fminf(tf, fmaxf(t0, t1));
+  }
+  return tn <= tf && tf >= s_min;
+}
+
+QM_HD float half_diagonal(const float4* b) { return sqrtf(b[1].w * b[1].w + b[2].w * b[2].w + b[3].w * b[3].w); }
+
+// axis: direction of travel toward the sun (not necessarily unit);
+// tan_theta: tangent of the largest angle between a sun-shape direction and
+// the axis.
+QM_HD bool shadow_free(const ShadowGrid& g, int own, float3 axis, float tan_theta) {
+  if (!(tan_theta >= 0.0f) || tan_theta > 0.5f) return false;
+  const float al = sqrtf(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
+  if (!(al > 0.0f)) return false;
+  const float3 a = make_float3(axis.x / al, axis.y / al, axis.z / al);
+  const float tq = tan_theta * sqrtf(1.0f + tan_theta * tan_theta) * 1.001f + 1e-6f;
+  const float4* bi = g.bound + 5 * own;
+  const float3 c = make_float3(bi[0].x, bi[0].y, bi[0].z);
+  const float ri = half_diagonal(bi);
+  const float margin = 0.05f + 2e-6f * (fabsf(c.x) + fabsf(c.y) + fabsf(c.z));
+  const float3 lo = g.pos;
+  const float3 hi = make_float3(g.pos.x + g.cells.x * g.interval.x, g.pos.y + g.cells.y * g.interval.y,
+                                g.pos.z + g.cells.z * g.interval.z);
+  const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+  // Longest axis run that can matter: inside the grid widened by the widest
+  // capsule radius.
+  const float s_max = sqrtf(dx * dx + dy * dy + dz * dz) + 4.0f * ri + 10.0f;
+  const float R = ri + (s_max + ri) * tq + margin;
+  float s_end = s_max;
+  {
+    // where the axis leaves the grid widened by R
+    float tn = -3.0e38f, tf = 3.0e38f;
+    const float ov[3] = {c.x, c.y, c.z}, dv[3] = {a.x, a.y, a.z};
+    const float lv[3] = {lo.x - R, lo.y - R, lo.z - R}, hv[3] = {hi.x + R, hi.y + R, hi.z + R};
+    for (int k = 0; k < 3; ++k) {
+      if (fabsf(dv[k]) < 1e-12f) {
+        if (ov[k] < lv[k] || ov[k] > hv[k]) return true;  // the capsule never meets the grid
+        continue;
+      }
+      const float t0 = (lv[k] - ov[k]) / dv[k], t1 = (hv[k] - ov[k]) / dv[k];
+      tn = fmaxf(tn, fminf(t0, t1));
+      tf = fminf(tf, fmaxf(t0, t1));
+    }
+    if (tf < -ri) return true;
+    s_end = fminf(s_end, tf);
+  }
+  const float s0 = -ri;
+  const float3 p0 = make_float3(c.x + s0 * a.x, c.y + s0 * a.y, c.z + s0 * a.z);
+  const float3 p1 = make_float3(c.x + s_end * a.x, c.y + s_end * a.y, c.z + s_end * a.z);
+  const float bmin[3] = {fminf(p0.x, p1.x) - R, fminf(p0.y, p1.y) - R, fminf(p0.z, p1.z) - R};
+  const float bmax[3] = {fmaxf(p0.x, p1.x) + R, fmaxf(p0.y, p1.y) + R, fmaxf(p0.z, p1.z) + R};
+  const float gp[3] = {lo.x, lo.y, lo.z}, gi[3] = {g.interval.x, g.interval.y, g.interval.z};
+  const int gc[3] = {g.cells.x, g.cells.y, g.cells.z};
+  int c0[3], c1[3];
+  long long count = 1;
+  for (int k = 0; k < 3; ++k) {
+    const float f0 = floorf((bmin[k] - gp[k]) / gi[k]), f1 = floorf((bmax[k] - gp[k]) / gi[k]);
+    if (f1 < 0.0f || f0 > (float)(gc[k] - 1)) return true;  // no cell of the grid
+    c0[k] = f0 < 0.0f ? 0 : (int)f0;
+    c1[k] = f1 > (float)(gc[k] - 1) ? gc[k] - 1 : (int)f1;
+    count *= (long long)(c1[k] - c0[k] + 1);
+  }
+  if (count > 8192) return false;  // too wide to be worth it: walk
+  for (int x = c0[0]; x <= c1[0]; ++x)
+    for (int y = c0[1]; y <= c1[1]; ++y)
+      for (int z = c0[2]; z <= c1[2]; ++z) {
+        const int cell = (x * gc[1] + y) * gc[2] + z;
+        const int2 rg = g.ranges[cell];
+        for (int k = rg.x; k < rg.y; ++k) {
+          const int j = g.entries[k].x;
+          if (j == own) continue;
+          const float4* bj = g.bound + 5 * j;
+          const float ex = bj[0].x - c.x, ey = bj[0].y - c.y, ez = bj[0].z - c.z;
+          const float D = sqrtf(ex * ex + ey * ey + ez * ez) + half_diagonal(bj);
+          const float w = ri + (D + ri) * tq + margin;
+          if (shadow_box_meets(bj, w, c, a, s0 - 1.0f)) return false;
+        }
+      }
+  return true;
+}
+
+}  // namespace qm

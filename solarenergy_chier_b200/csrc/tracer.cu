@@ -289,6 +289,7 @@ struct FacetWindow {
   // g in [0, P) plus a light index in [0, L) needs no wrap-around).
   const float4* samples[kThreads / 32];
   const float4* perturbations[kThreads / 32];
+  int shadow_free[kThreads / 32];  // the task's shadow walks can be skipped (qm::shadow_free)
   float4 o[kThreads];   // origin.xyz, pool offset g[f] (int bits)
   float4 u[kThreads];   // frame u.xyz, pool offset g[(f+1) % P] (int bits)
   float4 n[kThreads];   // frame n.xyz, frame identity flag
@@ -304,6 +305,13 @@ __device__ __forceinline__ float4 lds(const float4& x) {
   float4 r;
   const unsigned a = (unsigned)__cvta_generic_to_shared(&x);
   asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w) : "r"(a));
+  return r;
+}
+
+__device__ __forceinline__ int lds_int(const int& x) {
+  int r;
+  const unsigned a = (unsigned)__cvta_generic_to_shared(&x);
+  asm volatile("ld.shared.s32 %0, [%1];" : "=r"(r) : "r"(a));
   return r;
 }
 
@@ -380,6 +388,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   const DevGrid& G = p.grids[T.grid];
   const DevReceiver& R = p.receivers[T.receiver];
   if (lane == 0) {
+    win.shadow_free[threadIdx.x >> 5] = T.shadow_free;
     win.samples[threadIdx.x >> 5] = T.samples;
     win.perturbations[threadIdx.x >> 5] = T.perturbations;
   }
@@ -429,7 +438,10 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
       // frame (world space).
       const float3 dir = xyz(__ldg(lds_ptr(win.samples[threadIdx.x >> 5]) + __float_as_int(win.o[slot].w) + lab));
       int32_t code;
-      if (collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags)) {
+      // Heliostats whose rays no other heliostat can shadow skip the shadow
+      // walk (qm::shadow_free, decided per sun when the task is built).
+      if (!lds_int(win.shadow_free[threadIdx.x >> 5]) &&
+          collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags)) {
         code = kShadowed;
       } else {
         Frame nframe;

@@ -176,6 +176,12 @@ class Scene:
     def set_light_range(self, begin: int, end: int) -> None:
         check(self._lib.qmcrt_set_light_range(self._h, begin, end))
 
+    def shadow_free(self) -> np.ndarray:
+        """Per heliostat: 1 when its shadow walks are skipped for the current sun."""
+        f = np.zeros(self.num_heliostats, np.int32)
+        check(self._lib.qmcrt_debug_shadow_free(self._h, _ptr(f, ctypes.c_int)))
+        return f
+
     def set_sun(self, sun_dir) -> None:
         """Re-orient the field toward a new sun direction (direction of travel)."""
         d = np.ascontiguousarray(np.asarray(sun_dir, np.float32).reshape(3))

@@ -293,3 +293,34 @@ def test_set_sun_traces_like_a_scene_loaded_with_that_sun(tmp_path):
         got = c.scene.hit_records(h, 0, min(nf, 200), 0, L)
         want = o2.trace([h], c.dirs, c.pert, c.offsets, record=(h, 0, min(nf, 200)), images=False)["records"]
         assert np.array_equal(got, want), f"heliostat {h}: {np.mean(got != want):.2e} of rays differ"
+
+
+@pytest.mark.parametrize("sun", [[0.0, -0.866, -0.5], [0.2, -0.26, 0.94], [-0.9, -0.3, 0.3]])
+def test_shadow_skip_keeps_per_ray_outcomes(tmp_path, sun):
+    # Heliostats flagged shadow-free skip their shadow walks; at low suns some
+    # are shadowed and are not flagged.  Per-ray outcomes (exact build) must
+    # stay identical to the oracle's either way.
+    import json
+    from pathlib import Path
+
+    f = synth.large_field(tmp_path, seed=6, num_heliostats=40, helio_pixel=0.25, receiver_pixel=0.05, groups=4,
+                          per_group=128)
+    c = Case(f, seed=9)
+    cfg = json.loads(Path(f.config).read_text())
+    c2 = tmp_path / "sun.json"
+    c2.write_text(json.dumps(dict(cfg, sun_dir=sun)))
+    o2 = oracle.OracleScene.from_files(f.scene, c2)
+    c.scene.set_sun(sun)
+    c.scene.set_math_mode(True)
+    flags = c.scene.shadow_free()
+    L = c.scene.lights_per_group
+    shadowed = 0
+    for h in range(0, c.scene.num_heliostats, 3):
+        nf = c.scene.heliostat(h)["num_facets"]
+        got = c.scene.hit_records(h, 0, min(nf, 150), 0, L)
+        want = o2.trace([h], c.dirs, c.pert, c.offsets, record=(h, 0, min(nf, 150)), images=False)["records"]
+        assert np.array_equal(got, want), f"heliostat {h} (shadow-free {flags[h]}): {np.mean(got != want):.2e} differ"
+        if flags[h]:
+            assert not np.any(want == -1), f"heliostat {h} flagged shadow-free but the oracle shadows rays"
+        shadowed += int(np.sum(want == -1))
+    print("sun", sun, "shadow-free heliostats", int(flags.sum()), "of", len(flags), "shadowed rays", shadowed)
