@@ -156,6 +156,11 @@ int qmcrt_diagnostics(qmcrt_scene* scene, unsigned long long* out4);
  * (a conservative capsule test around the sun-shape cone; no reference
  * counterpart -- the reference walks every ray). */
 int qmcrt_debug_shadow_free(qmcrt_scene* scene, int* flags);
+/* Debug: per sub-heliostat of a grid (grid-local ids, as qmcrt_grid_vertices),
+ * 1 when the block walks of its facets are skipped because no other
+ * heliostat can block a ray reflected from it (same kind of test around its
+ * reflected cone). */
+int qmcrt_debug_block_free(qmcrt_scene* scene, int grid, int* flags);
 
 /* Per-ray outcome for facets [facet_begin, facet_end) x lights [light_begin,
  * light_end) of one heliostat, row-major by facet: pixel index for a

@@ -73,6 +73,7 @@ PROTOTYPES = {
     "qmcrt_diagnostics": (_i, [_vp, _pull]),
     "qmcrt_debug_hit_records": (_i, [_vp, _i, _i, _i, _i, _i, _pi]),
     "qmcrt_debug_shadow_free": (_i, [_vp, _pi]),
+    "qmcrt_debug_block_free": (_i, [_vp, _i, _pi]),
     "qmcrt_smooth": (_i, [_vp, _i, _i, _i, _f, _vp]),
     "qmcrt_smooth_static": (_i, [_vp, _i, _i, _i, _f, _vp]),
     "qmcrt_load_tasks": (_i, [_vp, ctypes.c_char_p, _pi, _pi, _i, _pi, _pi, _pi]),

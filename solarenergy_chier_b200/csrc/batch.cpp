@@ -60,11 +60,15 @@ void batch_prepare(qmcrt_batch* b, cudaStream_t st) {
     float3 axis;
     float tan_world;
     sun_cone(I.sun, I.scene->sun_shape_tan, axis, tan_world);
+    const float block_theta = tan_world < 0.0f || I.scene->slope_angle < 0.0f
+                                  ? -1.0f
+                                  : std::atan(tan_world) + 2.0f * I.scene->slope_angle;
     for (int h = 0; h < H; ++h) {
       qm::PrepItem& it = b->items[I.task_base + h];
       it.sun_dir = I.sun;
       it.shadow_axis = axis;
       it.shadow_tan = tan_world;
+      it.block_theta = block_theta;
     }
   }
   cuda_check(cudaMemcpyAsync(b->d_tasks.p, b->tasks.data(), b->tasks.size() * sizeof(qm::DevTask),
@@ -227,6 +231,7 @@ int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scen
     b->d_hsub.alloc(std::max<long long>(n_hsub, 1) * sizeof(int4));
     b->d_subv.alloc(std::max<long long>(3 * n_sub, 1) * sizeof(float4));
     b->d_verts.alloc(std::max<long long>(3 * n_sub, 1) * sizeof(float3));
+    b->d_sub_free.alloc(std::max<long long>(n_sub, 1) * sizeof(int));
     b->d_images.alloc(std::max<long long>(n_img, 1) * sizeof(float));
     b->d_power.alloc(std::max(n_power, 1) * sizeof(double));
     b->d_pools.alloc(std::max<long long>(n_pool, 1) * sizeof(float4));
@@ -238,6 +243,7 @@ int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scen
       b->grids[g].bound = b->d_bound.as<float4>() + grid_slot[g].bound;
       b->grids[g].hsub = b->d_hsub.as<int4>() + grid_slot[g].hsub;
       b->grids[g].subv = b->d_subv.as<float4>() + 3 * grid_slot[g].sub;
+      b->grids[g].sub_free = b->d_sub_free.as<int>() + grid_slot[g].sub;
     }
     for (size_t r = 0; r < b->receivers.size(); ++r) b->receivers[r].image = b->d_images.as<float>() + b->image_offset[r];
     for (const auto& I : b->inst)
@@ -249,6 +255,7 @@ int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scen
       const long long sub = gs.sub + it.sub_first;
       it.verts = b->d_verts.as<float3>() + 3 * sub;
       it.subv = b->d_subv.as<float4>() + 3 * sub;
+      it.sub_free = b->d_sub_free.as<int>() + sub;
       it.bound = b->d_bound.as<float4>() + gs.bound + 5 * item_slot[i].local;
       it.hsub = b->d_hsub.as<int4>() + gs.hsub + item_slot[i].local;
     }

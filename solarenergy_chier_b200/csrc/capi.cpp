@@ -152,6 +152,8 @@ void build_device_scene(qmcrt_scene* s) {
     upload(gb->bound, bound);
     upload(gb->hsub, hsub);
     upload(gb->subv, subv);
+    // block-free flags start cleared (no skipping) until the pools exist
+    upload(gb->sub_free, std::vector<int>(std::max(g.num_subheliostats, 1), 0));
     DevGrid dg;
     dg.pos = g.pos;
     dg.interval = g.interval;
@@ -162,6 +164,7 @@ void build_device_scene(qmcrt_scene* s) {
     dg.bound = gb->bound.as<float4>();
     dg.hsub = gb->hsub.as<int4>();
     dg.subv = gb->subv.as<float4>();
+    dg.sub_free = gb->sub_free.as<int>();
     s->grids.push_back(dg);
     s->grid_bufs.push_back(std::move(gb));
   }
@@ -257,33 +260,57 @@ void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world) {
   tan_world = tan_local < 0.0f ? -1.0f : (float)(tan_local / len);
 }
 
-// Shadow-free flags of every heliostat's template for the current sun and
-// pool (qm::shadow_free, csrc/shadow.h).
-void update_shadow_flags(qmcrt_scene* s) {
-  std::vector<float4> pool(s->pool_size);
-  cuda_check(cudaMemcpy(pool.data(), s->d_samples.p, pool.size() * sizeof(float4), cudaMemcpyDeviceToHost),
-             "pool readback");
+// Tangent of the largest angle between a pool direction and the pool's
+// local +y axis (-1 when some direction has y <= 0: unbounded).
+double pool_tan(const DBuf& pool, int n) {
+  std::vector<float4> v(n);
+  cuda_check(cudaMemcpy(v.data(), pool.p, v.size() * sizeof(float4), cudaMemcpyDeviceToHost), "pool readback");
   double tmax = 0.0;
-  for (const float4& q : pool) {
-    if (!(q.y > 0.0f)) {
-      tmax = -1.0;
-      break;
-    }
+  for (const float4& q : v) {
+    if (!(q.y > 0.0f)) return -1.0;
     tmax = std::max(tmax, std::sqrt((double)q.x * q.x + (double)q.z * q.z) / q.y);
   }
-  s->sun_shape_tan = (float)tmax;
+  return tmax;
+}
+
+// Walk-free flags for the current sun and pools (csrc/shadow.h): per
+// heliostat template for the shadow walks, per sub-heliostat for the block
+// walks.
+void update_shadow_flags(qmcrt_scene* s) {
+  s->sun_shape_tan = (float)pool_tan(s->d_samples, s->pool_size);
+  const double slope_tan = pool_tan(s->d_perturb, s->pool_size);
+  s->slope_angle = slope_tan < 0.0 ? -1.0f : (float)std::atan(slope_tan);
   float3 axis;
   float tan_world;
   sun_cone(s->model.config.sun_dir, s->sun_shape_tan, axis, tan_world);
+  const float block_theta =
+      tan_world < 0.0f || s->slope_angle < 0.0f ? -1.0f : std::atan(tan_world) + 2.0f * s->slope_angle;
   const qm::SceneModel& m = s->model;
-  for (size_t i = 0; i < m.heliostats.size(); ++i) {
-    const int g = m.heliostats[i].grid;
-    const qm::GridModel& gm = m.grids[g];
-    const GridBufs& gb = *s->grid_bufs[g];
-    qm::ShadowGrid view{gm.pos, gm.interval, gm.cells, gb.h_bound.data(), gb.h_ranges.data(), gb.h_entries.data()};
-    s->templates[i].shadow_free =
-        tan_world >= 0.0f && qm::shadow_free(view, (int)i - gm.start_heliostat, axis, tan_world) ? 1 : 0;
+  for (size_t gi = 0; gi < m.grids.size(); ++gi) {
+    const qm::GridModel& gm = m.grids[gi];
+    GridBufs& gb = *s->grid_bufs[gi];
+    const qm::ShadowGrid view{gm.pos, gm.interval, gm.cells, gb.h_bound.data(), gb.h_ranges.data(),
+                              gb.h_entries.data()};
+    std::vector<int> sub_free(std::max(gm.num_subheliostats, 1), 0);
+    for (int k = 0; k < gm.num_heliostats; ++k) {
+      const int i = gm.start_heliostat + k;
+      const qm::HeliostatModel& h = m.heliostats[i];
+      s->templates[i].shadow_free = tan_world >= 0.0f && qm::shadow_free(view, k, axis, tan_world) ? 1 : 0;
+      if (block_theta < 0.0f) continue;
+      const qm::Frame hf = qm::make_frame(h.normal, h.type == 1);
+      for (int sidx = 0; sidx < h.num_sub; ++sidx) {
+        const float3 n = h.type == 1 ? qm::to_world(hf, h.local_normals[sidx]) : h.normal;
+        sub_free[h.sub_begin + sidx] =
+            qm::block_free(view, k, gm.sub_vertices.data() + 3 * (size_t)(h.sub_begin + sidx),
+                           m.config.sun_dir, n, block_theta)
+                ? 1
+                : 0;
+      }
+    }
+    upload(gb.sub_free, sub_free);
+    s->grids[gi].sub_free = gb.sub_free.as<int>();
   }
+  upload(s->d_grids, s->grids);
   s->cache_valid = false;
 }
 
@@ -831,6 +858,18 @@ int qmcrt_debug_shadow_free(qmcrt_scene* s, int* flags) {
     checked(s);
     if (!flags) invalid("output is NULL");
     for (size_t i = 0; i < s->templates.size(); ++i) flags[i] = s->templates[i].shadow_free;
+  });
+}
+
+int qmcrt_debug_block_free(qmcrt_scene* s, int grid, int* flags) {
+  return guarded([&] {
+    checked(s);
+    if (!flags) invalid("output is NULL");
+    if (grid < 0 || grid >= (int)s->model.grids.size()) invalid("grid index out of range");
+    const int n = s->model.grids[grid].num_subheliostats;
+    DeviceGuard guard(s->device);
+    cuda_check(cudaMemcpy(flags, s->grid_bufs[grid]->sub_free.p, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost),
+               "flag readback");
   });
 }
 

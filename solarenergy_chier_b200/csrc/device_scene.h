@@ -20,6 +20,7 @@ struct DevGrid {
                         // for k = lattice x, normal, lattice z, then (x0, 1/px, z0, 1/pz)
   const int4* hsub;     // (first sub-heliostat id, count, lattice rows, lattice columns) per grid-local heliostat
   const float4* subv;   // 3 float4 per sub-heliostat: A.xyz AB.x | AB.yz AC.xy | AC.z
+  const int* sub_free;  // per sub-heliostat: 1 when its facets' block walks can be skipped (qm::block_free)
 };
 
 struct DevReceiver {

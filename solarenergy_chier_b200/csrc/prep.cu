@@ -70,6 +70,16 @@ __global__ void shadow_kernel(const PrepItem* items, int n, DevTask* tasks, cons
   const DevGrid& G = grids[T.grid];
   const ShadowGrid view{G.pos, G.interval, G.cells, G.bound, G.cell_range, G.entries};
   T.shadow_free = it.shadow_tan >= 0.0f && shadow_free(view, T.own, it.shadow_axis, it.shadow_tan) ? 1 : 0;
+  Frame hf;
+  hf.u = T.fu;
+  hf.n = T.fn;
+  hf.v = T.fv;
+  hf.identity = T.frame_identity != 0;
+  for (int s = 0; s < it.num_sub; ++s) {
+    const float3 n = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
+    it.sub_free[s] =
+        it.block_theta >= 0.0f && block_free(view, T.own, it.verts + 3 * s, it.sun_dir, n, it.block_theta) ? 1 : 0;
+  }
 }
 
 // Pool of instance blockIdx.y turned by that instance's sun frame.

@@ -26,6 +26,10 @@ struct PrepItem {
   // the largest sun-shape angle (< 0: unbounded, never shadow-free).
   float3 shadow_axis;
   float shadow_tan;
+  // Block-free test (qm::block_free): theta_sun + 2 theta_slope (< 0: never),
+  // and where the heliostat's per-sub-heliostat flags go.
+  float block_theta;
+  int* sub_free;
   float3* verts;    // out: 3 float3 (B, A, C) per sub-heliostat
   float4* subv;     // out: 3 float4 per sub-heliostat (A, B - A, C - A)
   float4* bound;    // out: 5 float4 traversal record

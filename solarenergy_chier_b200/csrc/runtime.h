@@ -84,7 +84,7 @@ void upload(DBuf& b, const std::vector<T>& v) {
 }
 
 struct GridBufs {
-  DBuf ranges, entries, bound, hsub, subv;
+  DBuf ranges, entries, bound, hsub, subv, sub_free;
   // host copies for the shadow-free test
   std::vector<float4> h_bound;
   std::vector<int2> h_ranges;
@@ -125,6 +125,7 @@ struct qmcrt_scene {
   std::vector<long long> offset_base;
   qrt::DBuf d_samples, d_perturb;
   float sun_shape_tan = -1.0f;  // tan of the largest sun-shape angle of the local pool (< 0: unbounded)
+  float slope_angle = -1.0f;    // largest angle of the slope-error pool from its axis, radians (< 0: unbounded)
   qrt::DBuf d_trace_samples;  // tracer copy: d_samples in world space, P + L entries (entry i = i % P)
   qrt::DBuf d_trace_perturb;  // tracer copy of d_perturb, P + L entries
   qrt::DBuf d_offset_seg;     // heliostats + 1 starts of the per-heliostat offset segments

@@ -1,5 +1,6 @@
-// Per-heliostat shadow-free test, shared by the host (plain scenes) and the
-// device (batch preparation).
+// Walk-free tests, shared by the host (plain scenes) and the device (batch
+// preparation): per heliostat for the shadow walks, per sub-heliostat for
+// the block walks.
 //
 // The reference walks every ray toward the sun through the grid
 // (rectGridDDA::collision, rectGridDDA.cu:31-119) and tests the
@@ -54,18 +55,15 @@ QM_HD bool shadow_box_meets(const float4* b, float w, float3 o, float3 a, float 
 
 QM_HD float half_diagonal(const float4* b) { return sqrtf(b[1].w * b[1].w + b[2].w * b[2].w + b[3].w * b[3].w); }
 
-// axis: direction of travel toward the sun (not necessarily unit);
-// tan_theta: tangent of the largest angle between a sun-shape direction and
-// the axis.
-QM_HD bool shadow_free(const ShadowGrid& g, int own, float3 axis, float tan_theta) {
-  if (!(tan_theta >= 0.0f) || tan_theta > 0.5f) return false;
+// Rays starting within ri of c, with directions within the angle whose
+// tangent is tan_theta of `axis` (not necessarily unit): true when none of
+// them can hit a heliostat other than `own` listed in a cell they can visit.
+QM_HD bool cone_free(const ShadowGrid& g, int own, float3 c, float ri, float3 axis, float tan_theta) {
+  if (!(tan_theta >= 0.0f) || tan_theta > 0.5f || !(ri >= 0.0f)) return false;
   const float al = sqrtf(axis.x * axis.x + axis.y * axis.y + axis.z * axis.z);
   if (!(al > 0.0f)) return false;
   const float3 a = make_float3(axis.x / al, axis.y / al, axis.z / al);
   const float tq = tan_theta * sqrtf(1.0f + tan_theta * tan_theta) * 1.001f + 1e-6f;
-  const float4* bi = g.bound + 5 * own;
-  const float3 c = make_float3(bi[0].x, bi[0].y, bi[0].z);
-  const float ri = half_diagonal(bi);
   const float margin = 0.05f + 2e-6f * (fabsf(c.x) + fabsf(c.y) + fabsf(c.z));
   const float3 lo = g.pos;
   const float3 hi = make_float3(g.pos.x + g.cells.x * g.interval.x, g.pos.y + g.cells.y * g.interval.y,
@@ -126,6 +124,39 @@ QM_HD bool shadow_free(const ShadowGrid& g, int own, float3 axis, float tan_thet
         }
       }
   return true;
+}
+
+// Shadow walks of heliostat `own`: its rays start on its facets, inside its
+// padded box; axis: direction of travel toward the sun; tan_theta: tangent
+// of the largest angle between a sun-shape direction and the axis.
+QM_HD bool shadow_free(const ShadowGrid& g, int own, float3 axis, float tan_theta) {
+  const float4* bi = g.bound + 5 * own;
+  return cone_free(g, own, make_float3(bi[0].x, bi[0].y, bi[0].z), half_diagonal(bi), axis, tan_theta);
+}
+
+// Block walks of the facets of one sub-heliostat (B, A, C as stored): its
+// facets lie on the parallelogram, within half its diagonal of its centre;
+// their reflected rays leave within theta_sun + 2 theta_slope of the mirror
+// image of the sun's direction of travel about the sub-heliostat's normal
+// (reflection keeps angles, and tilting the normal by d turns the reflected
+// ray by at most 2 d).  sun: the sun's direction of travel; normal: the
+// sub-heliostat's facet normal; theta: theta_sun + 2 theta_slope (radians).
+QM_HD bool block_free(const ShadowGrid& g, int own, const float3* bac, float3 sun, float3 normal, float theta) {
+  if (!(theta >= 0.0f) || theta > 0.45f) return false;
+  const float3 B = bac[0], A = bac[1], C = bac[2];
+  const float3 ab = make_float3(B.x - A.x, B.y - A.y, B.z - A.z), ac = make_float3(C.x - A.x, C.y - A.y, C.z - A.z);
+  const float3 c = make_float3(A.x + 0.5f * (ab.x + ac.x), A.y + 0.5f * (ab.y + ac.y), A.z + 0.5f * (ab.z + ac.z));
+  const float d1 = sqrtf((ab.x + ac.x) * (ab.x + ac.x) + (ab.y + ac.y) * (ab.y + ac.y) + (ab.z + ac.z) * (ab.z + ac.z));
+  const float d2 = sqrtf((ab.x - ac.x) * (ab.x - ac.x) + (ab.y - ac.y) * (ab.y - ac.y) + (ab.z - ac.z) * (ab.z - ac.z));
+  const float ri = 0.5f * fmaxf(d1, d2) + 0.01f;
+  const float sl = sqrtf(sun.x * sun.x + sun.y * sun.y + sun.z * sun.z);
+  const float nl = sqrtf(normal.x * normal.x + normal.y * normal.y + normal.z * normal.z);
+  if (!(sl > 0.0f) || !(nl > 0.0f)) return false;
+  const float3 s = make_float3(sun.x / sl, sun.y / sl, sun.z / sl), n = make_float3(normal.x / nl, normal.y / nl, normal.z / nl);
+  const float k = 2.0f * (s.x * n.x + s.y * n.y + s.z * n.z);
+  const float3 axis = make_float3(s.x - k * n.x, s.y - k * n.y, s.z - k * n.z);
+  // 1e-4 rad covers the float rounding of the axis and normals
+  return cone_free(g, own, c, ri, axis, tanf(theta + 1e-4f));
 }
 
 }  // namespace qm

@@ -291,7 +291,7 @@ struct FacetWindow {
   const float4* perturbations[kThreads / 32];
   int shadow_free[kThreads / 32];  // the task's shadow walks can be skipped (qm::shadow_free)
   float4 o[kThreads];   // origin.xyz, pool offset g[f] (int bits)
-  float4 u[kThreads];   // frame u.xyz, pool offset g[(f+1) % P] (int bits)
+  float4 u[kThreads];   // frame u.xyz, pool offset g[(f+1) % P] (int bits; bit 31: block walk skippable)
   float4 n[kThreads];   // frame n.xyz, frame identity flag
   float4 v[kThreads];   // frame v.xyz, walk start cell x (int bits)
   float4 lo[kThreads];  // walk start distances to the lower cell boundaries, cell y
@@ -420,7 +420,14 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         facet_geometry(T, fw, origin, fnormal);
         const Frame fr = qs::make_frame(fnormal, false);
         win.o[wbase + lane] = make_float4(origin.x, origin.y, origin.z, __int_as_float(__ldg(T.offsets + fw)));
-        win.u[wbase + lane] = make_float4(fr.u.x, fr.u.y, fr.u.z, __int_as_float(__ldg(T.offsets + (fw + 1) % T.pool_size)));
+        // Pool offsets lie below 2^30; bit 31 carries the facet's
+        // sub-heliostat block-free flag (qm::block_free).
+        const int per_row = T.row_col.y * T.sub_row_col.y;
+        const int block = T.type == 1 ? (fw / per_row / T.sub_row_col.x) * T.row_col.y + (fw % per_row) / T.sub_row_col.y
+                                      : 0;
+        const int free_bit = __ldg(G.sub_free + __ldg(&G.hsub[T.own].x) + block) ? (int)0x80000000 : 0;
+        win.u[wbase + lane] = make_float4(fr.u.x, fr.u.y, fr.u.z,
+                                          __int_as_float(__ldg(T.offsets + (fw + 1) % T.pool_size) | free_bit));
         win.n[wbase + lane] = make_float4(fr.n.x, fr.n.y, fr.n.z, fr.identity ? 1.0f : 0.0f);
         const WalkStart ws = walk_start(G, origin);
         win.v[wbase + lane] = make_float4(fr.v.x, fr.v.y, fr.v.z, __int_as_float(ws.cell.x));
@@ -450,10 +457,13 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         nframe.n = xyz(wn);
         nframe.v = xyz(win.v[slot]);
         nframe.identity = wn.w != 0.0f;
-        const int b = __float_as_int(lds(win.u[slot]).w) + lab;
+        const int g1 = __float_as_int(lds(win.u[slot]).w);
+        const int b = (g1 & 0x7fffffff) + lab;
         float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
         float3 rd = qs::normalize(qs::reflect(neg(dir), n));
-        if (collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags)) {
+        // Facets of sub-heliostats no other heliostat can block skip the
+        // block walk (qm::block_free, decided per sun with the pools).
+        if (g1 >= 0 && collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags)) {
           code = kBlocked;
         } else {
           float tt, uu, vv;

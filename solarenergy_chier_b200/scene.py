@@ -182,6 +182,12 @@ class Scene:
         check(self._lib.qmcrt_debug_shadow_free(self._h, _ptr(f, ctypes.c_int)))
         return f
 
+    def block_free(self, grid: int = 0) -> np.ndarray:
+        """Per sub-heliostat of a grid: 1 when its facets' block walks are skipped."""
+        f = np.zeros(max(self.grid(grid)["num_sub"], 1), np.int32)
+        check(self._lib.qmcrt_debug_block_free(self._h, grid, _ptr(f, ctypes.c_int)))
+        return f
+
     def set_sun(self, sun_dir) -> None:
         """Re-orient the field toward a new sun direction (direction of travel)."""
         d = np.ascontiguousarray(np.asarray(sun_dir, np.float32).reshape(3))

@@ -297,9 +297,10 @@ def test_set_sun_traces_like_a_scene_loaded_with_that_sun(tmp_path):
 
 @pytest.mark.parametrize("sun", [[0.0, -0.866, -0.5], [0.2, -0.26, 0.94], [-0.9, -0.3, 0.3]])
 def test_shadow_skip_keeps_per_ray_outcomes(tmp_path, sun):
-    # Heliostats flagged shadow-free skip their shadow walks; at low suns some
-    # are shadowed and are not flagged.  Per-ray outcomes (exact build) must
-    # stay identical to the oracle's either way.
+    # Heliostats flagged shadow-free skip their shadow walks and facets of
+    # sub-heliostats flagged block-free their block walks; at low suns some
+    # rays are shadowed or blocked and their heliostats are not flagged.
+    # Per-ray outcomes (exact build) must stay identical to the oracle's.
     import json
     from pathlib import Path
 
@@ -323,4 +324,6 @@ def test_shadow_skip_keeps_per_ray_outcomes(tmp_path, sun):
         if flags[h]:
             assert not np.any(want == -1), f"heliostat {h} flagged shadow-free but the oracle shadows rays"
         shadowed += int(np.sum(want == -1))
-    print("sun", sun, "shadow-free heliostats", int(flags.sum()), "of", len(flags), "shadowed rays", shadowed)
+    bfree = c.scene.block_free(0)
+    print("sun", sun, "shadow-free heliostats", int(flags.sum()), "of", len(flags), "shadowed rays", shadowed,
+          "block-free sub-heliostats", int(bfree.sum()), "of", len(bfree))
