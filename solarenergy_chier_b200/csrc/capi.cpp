@@ -1,7 +1,7 @@
 // C ABI (include/qmcrt.h) over the host scene model and the sm_100a kernels.
 #include "qmcrt.h"
 #include "helio_geom.h"
-#include "shadow.h"
+#include "prep.h"
 
 #include <cuda_runtime.h>
 
@@ -143,12 +143,9 @@ void build_device_scene(qmcrt_scene* s) {
     }
     upload(gb->ranges, ranges);
     upload(gb->entries, entries);
-    gb->h_ranges = ranges;
-    gb->h_entries = entries;
     std::vector<float4> bound, subv;
     std::vector<int4> hsub;
     grid_sun_data(m, g, bound, hsub, subv);
-    gb->h_bound = bound;
     upload(gb->bound, bound);
     upload(gb->hsub, hsub);
     upload(gb->subv, subv);
@@ -220,6 +217,7 @@ void build_device_scene(qmcrt_scene* s) {
   s->d_samples.alloc((size_t)P * sizeof(float4));
   s->d_perturb.alloc((size_t)P * sizeof(float4));
   s->d_trace_samples.alloc((size_t)(P + cfg.num_per_sunshape_group) * sizeof(float4));
+  s->d_scratch_word.alloc(sizeof(unsigned));
   s->d_trace_perturb.alloc((size_t)(P + cfg.num_per_sunshape_group) * sizeof(float4));
   {
     std::vector<long long> seg(s->offset_base);
@@ -261,69 +259,69 @@ void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world) {
 }
 
 // Tangent of the largest angle between a pool direction and the pool's
-// local +y axis (-1 when some direction has y <= 0: unbounded).
-double pool_tan(const DBuf& pool, int n) {
-  std::vector<float4> v(n);
-  cuda_check(cudaMemcpy(v.data(), pool.p, v.size() * sizeof(float4), cudaMemcpyDeviceToHost), "pool readback");
-  double tmax = 0.0;
-  for (const float4& q : v) {
-    if (!(q.y > 0.0f)) return -1.0;
-    tmax = std::max(tmax, std::sqrt((double)q.x * q.x + (double)q.z * q.z) / q.y);
-  }
-  return tmax;
+// local +y axis, reduced on the device (-1 when some direction has y <= 0:
+// unbounded).
+float pool_tan(qmcrt_scene* s, const DBuf& pool) {
+  cuda_check(cudaMemset(s->d_scratch_word.p, 0, sizeof(unsigned)), "cudaMemset");
+  cuda_check(qm::launch_pool_tan(pool.as<float4>(), s->pool_size, s->d_scratch_word.as<unsigned>(), 0), "pool bound");
+  unsigned bits = 0;
+  cuda_check(cudaMemcpy(&bits, s->d_scratch_word.p, sizeof(unsigned), cudaMemcpyDeviceToHost), "pool bound");
+  float t;
+  std::memcpy(&t, &bits, sizeof(t));
+  return std::isfinite(t) ? t : -1.0f;
 }
 
-// Walk-free flags for the current sun and pools (csrc/shadow.h): per
-// heliostat template for the shadow walks, per sub-heliostat for the block
-// walks.
-void update_shadow_flags(qmcrt_scene* s) {
-  s->sun_shape_tan = (float)pool_tan(s->d_samples, s->pool_size);
-  const double slope_tan = pool_tan(s->d_perturb, s->pool_size);
-  s->slope_angle = slope_tan < 0.0 ? -1.0f : (float)std::atan(slope_tan);
+// Walk-free flags (csrc/shadow.h) for the current sun and pools, computed on
+// the device: per heliostat template for the shadow walks, per sub-heliostat
+// (each grid's sub_free array) for the block walks.  Skipped when neither the
+// sun nor the pools' angular bounds changed since the last computation.
+void update_shadow_flags(qmcrt_scene* s, bool pools_changed) {
+  if (pools_changed || s->sun_shape_tan < -1.5f) {
+    s->sun_shape_tan = pool_tan(s, s->d_samples);
+    const float slope_tan = pool_tan(s, s->d_perturb);
+    s->slope_angle = slope_tan < 0.0f ? -1.0f : std::atan(slope_tan);
+  }
+  const float3 sun = s->model.config.sun_dir;
+  if (s->flags_valid && sun.x == s->flags_sun.x && sun.y == s->flags_sun.y && sun.z == s->flags_sun.z &&
+      s->sun_shape_tan == s->flags_tan && s->slope_angle == s->flags_slope)
+    return;
   float3 axis;
   float tan_world;
-  sun_cone(s->model.config.sun_dir, s->sun_shape_tan, axis, tan_world);
-  const float block_theta =
-      tan_world < 0.0f || s->slope_angle < 0.0f ? -1.0f : std::atan(tan_world) + 2.0f * s->slope_angle;
-  const qm::SceneModel& m = s->model;
-  for (size_t gi = 0; gi < m.grids.size(); ++gi) {
-    const qm::GridModel& gm = m.grids[gi];
-    GridBufs& gb = *s->grid_bufs[gi];
-    const qm::ShadowGrid view{gm.pos, gm.interval, gm.cells, gb.h_bound.data(), gb.h_ranges.data(),
-                              gb.h_entries.data()};
-    std::vector<int> sub_free(std::max(gm.num_subheliostats, 1), 0);
-    for (int k = 0; k < gm.num_heliostats; ++k) {
-      const int i = gm.start_heliostat + k;
-      const qm::HeliostatModel& h = m.heliostats[i];
-      s->templates[i].shadow_free = tan_world >= 0.0f && qm::shadow_free(view, k, axis, tan_world) ? 1 : 0;
-      if (block_theta < 0.0f) continue;
-      const qm::Frame hf = qm::make_frame(h.normal, h.type == 1);
-      for (int sidx = 0; sidx < h.num_sub; ++sidx) {
-        const float3 n = h.type == 1 ? qm::to_world(hf, h.local_normals[sidx]) : h.normal;
-        sub_free[h.sub_begin + sidx] =
-            qm::block_free(view, k, gm.sub_vertices.data() + 3 * (size_t)(h.sub_begin + sidx),
-                           m.config.sun_dir, n, block_theta)
-                ? 1
-                : 0;
-      }
-    }
-    upload(gb.sub_free, sub_free);
-    s->grids[gi].sub_free = gb.sub_free.as<int>();
-  }
-  upload(s->d_grids, s->grids);
+  sun_cone(sun, s->sun_shape_tan, axis, tan_world);
+  qm::WalkFlagParams p{};
+  upload(s->d_flag_tasks, s->templates);
+  s->d_flag_out.alloc(std::max<size_t>(s->templates.size(), 1) * sizeof(int));
+  p.tasks = s->d_flag_tasks.as<DevTask>();
+  p.n = (int)s->templates.size();
+  p.grids = s->d_grids.as<DevGrid>();
+  p.sun_axis = axis;
+  p.sun_tan = tan_world;
+  p.sun_dir = sun;
+  p.block_theta = tan_world < 0.0f || s->slope_angle < 0.0f ? -1.0f : std::atan(tan_world) + 2.0f * s->slope_angle;
+  p.shadow_out = s->d_flag_out.as<int>();
+  cuda_check(qm::launch_walk_flags(p, 0), "walk flags");
+  std::vector<int> flags(s->templates.size());
+  if (!flags.empty())
+    cuda_check(cudaMemcpy(flags.data(), s->d_flag_out.p, flags.size() * sizeof(int), cudaMemcpyDeviceToHost),
+               "walk flags");
+  for (size_t i = 0; i < flags.size(); ++i) s->templates[i].shadow_free = flags[i];
+  s->flags_valid = true;
+  s->flags_sun = sun;
+  s->flags_tan = s->sun_shape_tan;
+  s->flags_slope = s->slope_angle;
   s->cache_valid = false;
 }
 
 // The tracer's copies of the pools (world-space samples, P + L entries);
 // redone after every change of the pools or of the sun, with the
 // shadow-free flags that depend on both.
-void rotate_pool(qmcrt_scene* s) {
+void rotate_pool(qmcrt_scene* s, bool pools_changed) {
   const int n_out = s->pool_size + s->model.config.num_per_sunshape_group;
   cuda_check(qm::launch_trace_pools(s->d_samples.as<float4>(), s->d_perturb.as<float4>(), s->pool_size, n_out, s->sun,
                                     s->d_trace_samples.as<float4>(), s->d_trace_perturb.as<float4>(), 0),
              "pool rotation");
   cuda_check(cudaDeviceSynchronize(), "pool rotation");
-  update_shadow_flags(s);
+  update_shadow_flags(s, pools_changed);
 }
 
 void generate_pool(qmcrt_scene* s, unsigned seed, int sunshape, float half_angle) {
@@ -356,7 +354,7 @@ void generate_pool(qmcrt_scene* s, unsigned seed, int sunshape, float half_angle
   }
   cuda_check(qm::launch_pool(p, 0), "pool kernel");
   cuda_check(cudaDeviceSynchronize(), "pool kernel");
-  rotate_pool(s);
+  rotate_pool(s, true);
 }
 
 qmcrt_scene* checked(qmcrt_scene* s) {
@@ -646,7 +644,6 @@ int qmcrt_scene_set_sun(qmcrt_scene* s, const float* sun_dir) {
       std::vector<float4> bound, subv;
       std::vector<int4> hsub;
       grid_sun_data(s->model, s->model.grids[g], bound, hsub, subv);
-      s->grid_bufs[g]->h_bound = bound;
       upload(s->grid_bufs[g]->bound, bound);
       upload(s->grid_bufs[g]->hsub, hsub);
       upload(s->grid_bufs[g]->subv, subv);
@@ -656,7 +653,8 @@ int qmcrt_scene_set_sun(qmcrt_scene* s, const float* sun_dir) {
     }
     upload(s->d_grids, s->grids);
     build_templates(s);
-    rotate_pool(s);
+    s->flags_valid = false;
+    rotate_pool(s, false);
   });
 }
 
@@ -670,15 +668,18 @@ int qmcrt_set_sample_pool(qmcrt_scene* s, const float* dirs, const float* pertur
       invalid("pool shape must match the configuration's groups x lights-per-group");
     DeviceGuard guard(s->device);
     const int n = s->pool_size;
-    DBuf tmp;
-    tmp.alloc((size_t)n * 3 * sizeof(float));
+    // staging for both xyz pools, kept with the scene (allocated once)
+    DBuf& tmp = s->d_pool_stage;
+    tmp.alloc((size_t)n * 6 * sizeof(float));
+    float* stage_dirs = tmp.as<float>();
+    float* stage_pert = stage_dirs + (size_t)n * 3;
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    cuda_check(cudaMemcpy(tmp.p, dirs, (size_t)n * 3 * sizeof(float), kind), "pool upload");
-    cuda_check(qm::launch_xyz_to_float4(tmp.as<float>(), s->d_samples.as<float4>(), n, 0), "pool convert");
-    cuda_check(cudaMemcpy(tmp.p, perturb, (size_t)n * 3 * sizeof(float), kind), "pool upload");
-    cuda_check(qm::launch_xyz_to_float4(tmp.as<float>(), s->d_perturb.as<float4>(), n, 0), "pool convert");
+    cuda_check(cudaMemcpy(stage_dirs, dirs, (size_t)n * 3 * sizeof(float), kind), "pool upload");
+    cuda_check(cudaMemcpy(stage_pert, perturb, (size_t)n * 3 * sizeof(float), kind), "pool upload");
+    cuda_check(qm::launch_xyz_to_float4(stage_dirs, s->d_samples.as<float4>(), n, 0), "pool convert");
+    cuda_check(qm::launch_xyz_to_float4(stage_pert, s->d_perturb.as<float4>(), n, 0), "pool convert");
     cuda_check(cudaDeviceSynchronize(), "pool convert");
-    rotate_pool(s);
+    rotate_pool(s, true);
   });
 }
 

@@ -119,6 +119,19 @@ __global__ void trace_pools_kernel(const float4* in, const float4* pert, int n, 
   out[i] = make_float4(d.x, d.y, d.z, 0.0f);
 }
 
+// Largest tan(angle from +y) of a pool, as float bits (non-negative floats
+// order like their bit patterns); +inf when some direction has y <= 0.
+__global__ void pool_tan_kernel(const float4* pool, int n, unsigned* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float t = 0.0f;
+  if (i < n) {
+    const float4 q = pool[i];
+    t = q.y > 0.0f ? sqrtf(q.x * q.x + q.z * q.z) / q.y : __int_as_float(0x7f800000);
+  }
+  for (int off = 16; off > 0; off >>= 1) t = fmaxf(t, __shfl_down_sync(0xffffffffu, t, off));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(t));
+}
+
 __global__ void xyz_to_float4_kernel(const float* xyz, float4* out, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -150,6 +163,12 @@ cudaError_t launch_trace_pools(const float4* samples, const float4* perturbation
                                const SunFrame& sun, float4* out, float4* pert_out, cudaStream_t stream) {
   if (n <= 0 || n_out <= 0) return cudaSuccess;
   trace_pools_kernel<<<(n_out + 255) / 256, 256, 0, stream>>>(samples, perturbations, n, n_out, sun, out, pert_out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pool_tan(const float4* pool, int n, unsigned* out, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  pool_tan_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pool, n, out);
   return cudaGetLastError();
 }
 

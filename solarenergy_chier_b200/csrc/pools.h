@@ -45,6 +45,9 @@ struct PoolParams {
 cudaError_t launch_pool(const PoolParams& p, cudaStream_t stream);
 cudaError_t launch_offsets(int* out, long long count, uint32_t seed, int heliostat, int pool, cudaStream_t stream);
 cudaError_t launch_xyz_to_float4(const float* xyz, float4* out, int n, cudaStream_t stream);
+// *out (zeroed by the caller) = bits of the largest tan(angle from +y) over
+// the pool (+inf if some direction has y <= 0).
+cudaError_t launch_pool_tan(const float4* pool, int n, unsigned* out, cudaStream_t stream);
 // Offsets of all heliostats; seg (device) holds heliostats + 1 segment starts.
 cudaError_t launch_offsets_all(int* out, const long long* seg, int heliostats, long long total, uint32_t seed, int pool,
                                cudaStream_t stream);

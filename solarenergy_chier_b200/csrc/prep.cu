@@ -82,6 +82,33 @@ __global__ void shadow_kernel(const PrepItem* items, int n, DevTask* tasks, cons
   }
 }
 
+// Walk-free flags of a plain scene's heliostats (its task templates); the
+// sub-heliostat parallelograms are read back from the traversal form
+// (A, B - A, C - A) -- the tests are conservative far above that rounding.
+__global__ void walk_flags_kernel(WalkFlagParams p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.n) return;
+  const DevTask& T = p.tasks[i];
+  const DevGrid& G = p.grids[T.grid];
+  const ShadowGrid view{G.pos, G.interval, G.cells, G.bound, G.cell_range, G.entries};
+  p.shadow_out[i] = p.sun_tan >= 0.0f && shadow_free(view, T.own, p.sun_axis, p.sun_tan) ? 1 : 0;
+  const int4 hs = G.hsub[T.own];
+  Frame hf;
+  hf.u = T.fu;
+  hf.n = T.fn;
+  hf.v = T.fv;
+  hf.identity = T.frame_identity != 0;
+  int* sub_free = const_cast<int*>(G.sub_free);
+  for (int s = 0; s < hs.y; ++s) {
+    const float4* q = G.subv + 3 * (hs.x + s);
+    const float3 A = make_float3(q[0].x, q[0].y, q[0].z);
+    const float3 bac[3] = {make_float3(A.x + q[0].w, A.y + q[1].x, A.z + q[1].y), A,
+                           make_float3(A.x + q[1].z, A.y + q[1].w, A.z + q[2].x)};
+    const float3 n = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
+    sub_free[hs.x + s] = p.block_theta >= 0.0f && block_free(view, T.own, bac, p.sun_dir, n, p.block_theta) ? 1 : 0;
+  }
+}
+
 // Pool of instance blockIdx.y turned by that instance's sun frame.
 __global__ void rotate_pools_kernel(const PoolRotation* jobs) {
   const PoolRotation J = jobs[blockIdx.y];
@@ -112,6 +139,12 @@ cudaError_t launch_shadow_flags(const PrepItem* items, int n, DevTask* tasks, co
                                 cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   shadow_kernel<<<(n + 127) / 128, 128, 0, stream>>>(items, n, tasks, grids);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_walk_flags(const WalkFlagParams& p, cudaStream_t stream) {
+  if (p.n <= 0) return cudaSuccess;
+  walk_flags_kernel<<<(p.n + 63) / 64, 64, 0, stream>>>(p);
   return cudaGetLastError();
 }
 

@@ -43,6 +43,20 @@ struct PoolRotation {
   SunFrame sun;
 };
 
+// Walk-free flags of a plain scene: shadow flags per task into shadow_out,
+// block flags per sub-heliostat into each grid's sub_free array.
+struct WalkFlagParams {
+  const DevTask* tasks;
+  int n;
+  const DevGrid* grids;
+  float3 sun_axis;  // toward the sun
+  float sun_tan;    // tan of the largest sun-shape angle (< 0: unbounded)
+  float3 sun_dir;   // direction of travel
+  float block_theta;
+  int* shadow_out;
+};
+cudaError_t launch_walk_flags(const WalkFlagParams& p, cudaStream_t stream);
+
 cudaError_t launch_prep(const PrepItem* items, int n, DevTask* tasks, cudaStream_t stream);
 // Shadow-free flags of the prepared tasks; grids: the tasks' grids with their
 // prepared traversal records.  Run after launch_prep.

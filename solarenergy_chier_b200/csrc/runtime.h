@@ -85,10 +85,6 @@ void upload(DBuf& b, const std::vector<T>& v) {
 
 struct GridBufs {
   DBuf ranges, entries, bound, hsub, subv, sub_free;
-  // host copies for the shadow-free test
-  std::vector<float4> h_bound;
-  std::vector<int2> h_ranges;
-  std::vector<int4> h_entries;
 };
 
 class DeviceGuard {
@@ -124,8 +120,14 @@ struct qmcrt_scene {
   qrt::DBuf d_offsets;
   std::vector<long long> offset_base;
   qrt::DBuf d_samples, d_perturb;
-  float sun_shape_tan = -1.0f;  // tan of the largest sun-shape angle of the local pool (< 0: unbounded)
+  float sun_shape_tan = -2.0f;  // tan of the largest sun-shape angle of the local pool (-1: unbounded, -2: unknown)
   float slope_angle = -1.0f;    // largest angle of the slope-error pool from its axis, radians (< 0: unbounded)
+  // walk-free flags: inputs of the last computation, device scratch
+  bool flags_valid = false;
+  float3 flags_sun{};
+  float flags_tan = 0.f, flags_slope = 0.f;
+  qrt::DBuf d_flag_tasks, d_flag_out, d_scratch_word;
+  qrt::DBuf d_pool_stage;  // staging of qmcrt_set_sample_pool uploads
   qrt::DBuf d_trace_samples;  // tracer copy: d_samples in world space, P + L entries (entry i = i % P)
   qrt::DBuf d_trace_perturb;  // tracer copy of d_perturb, P + L entries
   qrt::DBuf d_offset_seg;     // heliostats + 1 starts of the per-heliostat offset segments
@@ -163,6 +165,10 @@ struct qmcrt_scene {
     d_samples.release();
     d_perturb.release();
     d_trace_samples.release();
+    d_flag_tasks.release();
+    d_flag_out.release();
+    d_scratch_word.release();
+    d_pool_stage.release();
     d_trace_perturb.release();
     d_offset_seg.release();
     d_power.release();
