@@ -327,3 +327,44 @@ def test_shadow_skip_keeps_per_ray_outcomes(tmp_path, sun):
     bfree = c.scene.block_free(0)
     print("sun", sun, "shadow-free heliostats", int(flags.sum()), "of", len(flags), "shadowed rays", shadowed,
           "block-free sub-heliostats", int(bfree.sum()), "of", len(bfree))
+
+
+def test_sharded_trace_one_rank_equals_plain(small):
+    """shard.ShardedTrace over a one-rank NCCL group: the collectives run on
+    the tracer's own device image (a zero-copy view) and give the plain trace."""
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    from solarenergy_chier_b200 import shard
+
+    s = small.scene
+    ids = list(range(s.num_heliostats))
+    small.reset()
+    s.set_light_range(0, 8)
+    s.trace(ids)
+    want_img, (want_per, want_total) = s.image(0), s.power()
+    small.reset()
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        port = sock.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        st = shard.ShardedTrace(s, split="lights")
+        assert st.share(ids) == (ids, (0, s.lights_per_group))
+        s.set_light_range(0, 8)
+        s.trace(ids)  # the one-rank share of an 8-light trace
+        images, per, total = shard.reduce_flux([shard.device_image_tensor(s, 0)],
+                                               torch.from_numpy(s.power()[0]).cuda())
+        assert np.array_equal(images[0].cpu().numpy(), want_img)
+        assert np.array_equal(per.cpu().numpy(), want_per)
+        assert total == want_total
+        small.reset()
+        st.trace(ids)
+        images, per, total = st.reduce()
+        s.set_light_range(0, 8)
+        assert float(images[0].sum()) > float(want_img.sum())  # all lights traced
+    finally:
+        dist.destroy_process_group()
+        small.reset()
