@@ -20,11 +20,18 @@ Multi-GPU (torchrun): every rank traces the full field for its own light
 ranges (weak scaling, no collective inside the timed region); time is the
 maximum over ranks.
 
-`batched` (--batched-lights, default 4 light indexes per sun) compares, over
-96 sun positions (12 days x 8 hours, elevations 15-80 deg), the plain path
-looped over the suns with one batch traced by a single CUDA-graph launch.
+`batched` (--batched-lights, default 4 light indexes per instance) compares,
+over 96 sun positions of the field (12 days x 8 hours, elevations 15-80 deg)
+plus 16 seeded fields of uneven size at their own suns, the plain path
+looped over the instances with one batch traced by a single CUDA-graph
+launch.
 `adjoint` (--adjoint-lights, default 32) times the differentiable forward and
 its adjoint (aim-point optimisation set-up) on the field.
+`large_adjoint` (--large-adjoint-lights N, default 0 = skipped) times one
+forward + adjoint over 32 suns of a 10,000-heliostat field.
+`aim_optimisation` (--adam-steps K, default 0 = skipped) runs K Adam steps
+of aim-point optimisation on the field's 624 x 2 aim offsets, each step
+checked by the plain tracer on the same parameters.
 `reference_cuda` (--reference-cuda N) times the reference's own CUDA build
 on N heliostats spread over the field, and this tracer on the same ones.
 
@@ -64,6 +71,11 @@ def parse_args():
                    help="light indexes of the adjoint/forward cost comparison (0 = skip)")
     p.add_argument("--batched-lights", type=int, default=4,
                    help="light indexes per sun of the 96-sun batched-vs-plain comparison (0 = skip)")
+    p.add_argument("--adam-steps", type=int, default=0,
+                   help="Adam steps of aim-point optimisation, each checked by the plain tracer (0 = skip)")
+    p.add_argument("--adam-lights", type=int, default=8, help="light indexes per facet of each Adam step")
+    p.add_argument("--large-adjoint-lights", type=int, default=0,
+                   help="light indexes per sun of the 10,000-heliostat, 32-sun forward + adjoint (0 = skip)")
     p.add_argument("--impl", default="native", choices=["native", "reference"])
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -165,13 +177,18 @@ def census(files, lights: int = 8, stride: int = 4001):
     return per
 
 
-def batched_vs_plain(torch, scene, lights: int, stream):
-    """96 sun positions (12 days x 8 hours) of the field, `lights` light
-    indexes per facet per sun: the plain path looped over the suns (set_sun,
-    clear, one trace launch, image + FP64 power read back per sun) against one
-    batch (device-side preparation of all suns, one CUDA-graph launch that
-    clears and traces every sun, the same read-backs).  CUDA events on one
-    stream around each whole loop; the scene's own sun is restored after."""
+def batched_vs_plain(torch, scene, lights: int, stream, num_fields: int = 16, seed: int = 0):
+    """96 sun positions (12 days x 8 hours) of the field plus `num_fields`
+    seeded fields of uneven size (synth.uneven_field: 200-2500 heliostats,
+    6-12 m squares, rectangle or cylinder receivers) at their own suns,
+    `lights` light indexes per facet per instance: the plain path looped over
+    the instances (set_sun, clear, one trace launch, image + FP64 power read
+    back per instance) against one batch (device-side preparation of every
+    instance, one CUDA-graph launch that clears and traces them all, the same
+    read-backs).  CUDA events on one stream around each whole loop; the
+    scene's own sun is restored after."""
+    import tempfile
+
     import numpy as np
 
     import solarenergy_chier_b200 as q
@@ -179,39 +196,47 @@ def batched_vs_plain(torch, scene, lights: int, stream):
 
     suns = synth.sun_positions()
     own_sun = np.array(scene.info.sun_dir[:], np.float32)
-    ids = list(range(scene.num_heliostats))
-    nf = sum(scene.heliostat(h)["num_facets"] for h in ids)
-    rays = nf * lights * len(suns)
-    scene.set_light_range(0, lights)
+    tmp = Path(tempfile.mkdtemp(prefix="qmcrt_fields_"))
+    fields = [q.Scene(f.scene, f.config, device=torch.cuda.current_device(), seed=seed + 17 + k)
+              for k, f in enumerate(synth.uneven_field(tmp, k, seed=seed) for k in range(num_fields))]
+    # (scene, sun, heliostat ids) of every instance
+    work = [(scene, sun) for sun in suns] + [(f, np.array(f.info.sun_dir[:], np.float32)) for f in fields]
+    ids = {id(sc): list(range(sc.num_heliostats)) for sc in [scene] + fields}
+    facets = {id(sc): sum(sc.heliostat(h)["num_facets"] for h in ids[id(sc)]) for sc in [scene] + fields}
+    rays = sum(facets[id(sc)] for sc, _ in work) * lights
+    for sc in [scene] + fields:
+        sc.set_light_range(0, lights)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def plain_loop(sun_list):
-        for sun in sun_list:
-            scene.set_sun(sun)
-            scene.clear(stream=stream)
-            scene.clear_power()
-            scene.trace(ids, stream)
-            scene.image(0)
-            scene.power()
+    def plain_loop(items):
+        for sc, sun in items:
+            sc.set_sun(sun)
+            sc.clear(stream=stream)
+            sc.clear_power()
+            sc.trace(ids[id(sc)], stream)
+            sc.image(0)
+            sc.power()
 
-    plain_loop(suns[:2])  # warm-up
+    plain_loop(work[:2] + work[-2:])  # warm-up
     torch.cuda.synchronize()
     e0.record(stream)
-    plain_loop(suns)
+    plain_loop(work)
     e1.record(stream)
     torch.cuda.synchronize()
     plain_ms = e0.elapsed_time(e1)
 
-    batch = q.Batch([scene], [(0, s) for s in suns])
+    scenes = [scene] + fields
+    inst = [(0, sun) for sun in suns] + [(1 + k, sun) for k, (_, sun) in enumerate(work[len(suns):])]
+    batch = q.Batch(scenes, inst)
     batch.set_light_range(0, lights)
     mode, _ = batch.autotune(stream)
     batch.capture_graph(clear_first=True)
     batch.graph_launch(stream)  # warm-up
     torch.cuda.synchronize()
     e0.record(stream)
-    batch.set_suns(suns, stream)
+    batch.set_suns([sun for _, sun in inst], stream)
     batch.graph_launch(stream)
-    for k in range(len(suns)):
+    for k in range(len(inst)):
         batch.image(k)
         batch.power(k)
     e1.record(stream)
@@ -223,8 +248,12 @@ def batched_vs_plain(torch, scene, lights: int, stream):
     torch.cuda.synchronize()
     kernel_ms = e0.elapsed_time(e1)
     batch.close()
+    for f in fields:
+        f.close()
     scene.set_sun(own_sun)
-    return {"suns": len(suns), "lights_per_sun": lights, "rays": rays, "autotuned_mode": mode,
+    return {"suns": len(suns), "fields": num_fields,
+            "field_heliostats": [f.num_heliostats for f in fields], "lights_per_instance": lights, "rays": rays,
+            "autotuned_mode": mode,
             "plain_looped_mrays_s": rays / (plain_ms / 1e3) / 1e6, "batched_mrays_s": rays / (batched_ms / 1e3) / 1e6,
             "batched_graph_only_mrays_s": rays / (kernel_ms / 1e3) / 1e6,
             "speedup_batched_vs_plain": plain_ms / batched_ms, "plain_ms": plain_ms, "batched_ms": batched_ms}
@@ -241,18 +270,15 @@ def adjoint_vs_forward(torch, scene, lights: int, stream):
 
     import solarenergy_chier_b200 as q
 
+    from solarenergy_chier_b200 import aim
+
     d = q.Diff(scene, 2.0)
     d.set_light_range(0, lights)
     r = scene.receiver(0)
-    rows, cols = np.mgrid[0:r["height"], 0:r["width"]]
     d.set_target(np.zeros((r["height"], r["width"]), np.float32))
     d.forward(stream)
-    f0 = d.flux(0)
-    lit = f0 > 0.05 * f0.max()
+    d.set_target(aim.smooth_target(d.flux(0), seed=7))
     rng = np.random.default_rng(7)
-    ph = rng.uniform(0, 2 * np.pi, 2)
-    bump = 1.0 + 0.5 * np.cos(2 * np.pi * cols / r["width"] * 3 + ph[0]) * np.cos(np.pi * rows / r["height"] + ph[1])
-    d.set_target((bump * lit * f0[lit].mean()).astype(np.float32))
     H = scene.num_heliostats
     d.set_params(rng.uniform(-0.5, 0.5, (H, 2)), rng.uniform(-5e-4, 5e-4, (H, 2)))
     for _ in range(2):
@@ -280,6 +306,95 @@ def adjoint_vs_forward(torch, scene, lights: int, stream):
     return {"lights": lights, "forward_ms": fwd, "adjoint_ms": bwd, "adjoint_over_forward": bwd / fwd,
             "plain_trace_ms": plain, "forward_over_plain": fwd / plain, "loss": loss,
             "grad_norm": float(np.linalg.norm(grad)), "sigma_px": 2.0}
+
+
+def aim_optimisation(torch, scene, steps: int, lights: int, stream):
+    """Adam on the field's 624 x 2 aim offsets (uniform +-1 m start) toward a
+    smooth seeded target (peak/mean <= 2), `lights` light indexes per facet,
+    every step checked by the plain tracer on the same parameters
+    (solarenergy_chier_b200.aim).  Reports the loss and the plain tracer's
+    loss at the start and end, the worst forward-vs-plain power difference and
+    the worst splat-vs-plain flux L1 over the steps, and the time per step."""
+    import numpy as np
+
+    import solarenergy_chier_b200 as q
+    from solarenergy_chier_b200 import aim
+
+    d = q.Diff(scene, 2.0)
+    d.set_light_range(0, lights)
+    r = scene.receiver(0)
+    d.set_target(np.zeros((r["height"], r["width"]), np.float32))
+    d.forward(stream)
+    target = aim.smooth_target(d.flux(0), seed=7)
+    d.set_target(target)
+    H = scene.num_heliostats
+    rng = np.random.default_rng(11)
+    t0 = time.perf_counter()
+    res = aim.optimise_aim(d, target, steps=steps, lr_aim=0.05, aim0=rng.uniform(-1.0, 1.0, (H, 2)), check=True,
+                           cylinder=r["type"] == 1, stream=stream)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    d.close()
+    h = res.history
+    return {"steps": steps, "lights": lights, "parameters": H * 2, "loss_first": h[0]["loss"],
+            "loss_last": h[-1]["loss"], "plain_loss_first": h[0]["plain_loss"], "plain_loss_last": h[-1]["plain_loss"],
+            "max_power_rel_diff_fwd_vs_plain": max(abs(x["power"] - x["plain_power"]) / x["plain_power"] for x in h),
+            "max_splat_vs_plain_l1": max(x["plain_vs_splat_l1"] for x in h), "s_per_step_with_check": wall / steps}
+
+
+def large_adjoint(torch, lights: int, num_suns: int, stream, seed: int = 0):
+    """Forward plus adjoint of one pair over `num_suns` sun positions of the
+    10,000-heliostat field (synth.huge_field: flat 10x10 m heliostats,
+    0.05 m micro-facets = 40,000 per heliostat, 150-1800 m, cylinder r 10 m,
+    h 20 m at 200 m), `lights` light indexes per facet per sun, gradient with
+    respect to the 10,000 x 2 aim offsets (and normal offsets), hit records
+    checkpointed or recomputed as the free memory decides.  CUDA events
+    around one forward and one adjoint after a warm-up pair."""
+    import numpy as np
+
+    import solarenergy_chier_b200 as q
+    from solarenergy_chier_b200 import aim, synth
+
+    files = synth.huge_field(Path(tempfile.mkdtemp(prefix="qmcrt_huge_")), seed=seed)
+    scene = q.Scene(files.scene, files.config, device=torch.cuda.current_device(), seed=seed + 3)
+    H = scene.num_heliostats
+    facets = sum(scene.heliostat(h)["num_facets"] for h in range(H))
+    suns = synth.sun_positions()[:: max(1, 96 // num_suns)][:num_suns]
+    d = q.Diff(scene, 2.0, suns=suns)
+    d.set_light_range(0, lights)
+    r = scene.receiver(0)
+    zero = np.zeros((r["height"], r["width"]), np.float32)
+    for k in range(len(suns)):
+        d.set_target(zero, receiver=k)
+    d.forward(stream)
+    for k in range(len(suns)):
+        d.set_target(aim.smooth_target(d.flux(k), seed=100 + k), receiver=k)
+    rng = np.random.default_rng(5)
+    d.set_params(rng.uniform(-1.0, 1.0, (H, 2)), rng.uniform(-1e-3, 1e-3, (H, 2)))
+    d.forward(stream)
+    d.backward(stream)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record(stream)
+    loss = d.forward(stream)
+    e[1].record(stream)
+    grad = d.backward(stream)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    fwd, bwd = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+    free_b, total_b = torch.cuda.mem_get_info()
+    used = int(total_b - free_b)
+    recomputed, ckpt = d.hit_records()
+    rays = facets * lights * len(suns)
+    out = {"heliostats": H, "facets_per_heliostat": facets // H, "suns": len(suns), "lights_per_sun": lights,
+           "rays_per_sun": facets * lights, "rays": rays, "forward_ms": fwd, "adjoint_ms": bwd,
+           "adjoint_over_forward": bwd / fwd, "forward_mrays_s": rays / (fwd / 1e3) / 1e6,
+           "hit_records": "recomputed" if recomputed else "checkpointed", "checkpoint_bytes": ckpt,
+           "device_memory_used_bytes": used,
+           "loss": loss, "grad_norm": float(np.linalg.norm(grad))}
+    d.close()
+    scene.close()
+    return out
 
 
 def cpu_baseline(files, seconds: float):
@@ -491,6 +606,10 @@ def main():
             line["batched"] = batched_vs_plain(torch, scene, args.batched_lights, stream)
         if args.adjoint_lights > 0:
             line["adjoint"] = adjoint_vs_forward(torch, scene, args.adjoint_lights, stream)
+        if args.large_adjoint_lights > 0:
+            line["large_adjoint"] = large_adjoint(torch, args.large_adjoint_lights, 32, stream)
+        if args.adam_steps > 0:
+            line["aim_optimisation"] = aim_optimisation(torch, scene, args.adam_steps, args.adam_lights, stream)
         if args.reference_cuda > 0:
             line["reference_cuda"] = reference_cuda(files, scene, args.reference_cuda)
         if not args.no_cpu_baseline:

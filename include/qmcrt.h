@@ -227,7 +227,23 @@ int qmcrt_batch_debug_geometry(qmcrt_batch* batch, int instance, int grid, float
  * offsets are reused by every forward. */
 typedef struct qmcrt_diff qmcrt_diff;
 int qmcrt_diff_create(qmcrt_scene* scene, float sigma_px, qmcrt_diff** out);
+/* The pair over n_suns suns of one scene (sun_dirs: 3 floats each, direction
+ * of travel), traced by one launch.  The parameters are shared by every sun
+ * (each heliostat has one aim point and one normal offset); receiver indexes
+ * of the target / flux / image calls run over the suns' receivers
+ * (k x num_receivers + r for receiver r at sun k); the loss sums over all;
+ * qmcrt_bwd and qmcrt_diff_power sum over the suns per heliostat. */
+int qmcrt_diff_create_suns(qmcrt_scene* scene, const float* sun_dirs, int n_suns, float sigma_px, qmcrt_diff** out);
 void qmcrt_diff_free(qmcrt_diff* diff);
+/* Hit records of the forward for the adjoint: mode 0 chooses (checkpoint
+ * while rays / 8 bytes fit in a quarter of the free device memory, else
+ * recompute), 1 checkpoints them, 2 recomputes them in the adjoint with a
+ * hit-bit trace of each segment of segment_rays rays (0 keeps the current
+ * size; default 2^28 rays) before its adjoint launch.  Both give the same
+ * gradient.  qmcrt_diff_hit_records reports the last forward's choice and
+ * the checkpoint's size. */
+int qmcrt_diff_set_hit_records(qmcrt_diff* diff, int mode, long long segment_rays);
+int qmcrt_diff_hit_records(qmcrt_diff* diff, int* recomputed, long long* checkpoint_bytes);
 /* aim_offsets, normal_offsets: 2 floats per heliostat each (NULL = zeros). */
 int qmcrt_diff_set_params(qmcrt_diff* diff, const float* aim_offsets, const float* normal_offsets);
 int qmcrt_diff_set_target(qmcrt_diff* diff, int receiver, const float* target);
@@ -236,6 +252,18 @@ int qmcrt_fwd(qmcrt_diff* diff, double* loss, void* stream);
 int qmcrt_bwd(qmcrt_diff* diff, double* grad, void* stream);
 /* The smoothed flux F of the last forward. */
 int qmcrt_diff_flux(qmcrt_diff* diff, int receiver, float* out, int* width, int* height);
+/* The plain tracer on the pair's current parameters: the same rays as the
+ * forward, each hit's energy added to its nearest pixel (as
+ * qmcrt_trace_heliostats), into the images and powers that qmcrt_diff_image
+ * and qmcrt_diff_power read.  A pending qmcrt_bwd stays valid.  Used to check
+ * an optimisation step against the tracer the reference runs. */
+int qmcrt_diff_plain(qmcrt_diff* diff, void* stream);
+/* Unsmoothed flux of the last trace: after qmcrt_fwd the bilinear deposit
+ * (FP64, rounded to float), after qmcrt_diff_plain the plain flux. */
+int qmcrt_diff_image(qmcrt_diff* diff, int receiver, float* out, int* width, int* height);
+/* FP64 per-heliostat powers and their compensated total of the last trace
+ * (forward or plain; equal up to summation order for the same parameters). */
+int qmcrt_diff_power(qmcrt_diff* diff, double* per_heliostat, double* total);
 
 /* ---- smoothing and output ------------------------------------------------
  * Replaces ImageSmoother::image_smooth (Tool/Smoother/ImageSmoother.cu:68-113):

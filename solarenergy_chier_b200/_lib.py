@@ -101,6 +101,12 @@ PROTOTYPES = {
     "qmcrt_fwd": (_i, [_vp, _pd, _vp]),
     "qmcrt_bwd": (_i, [_vp, _pd, _vp]),
     "qmcrt_diff_flux": (_i, [_vp, _i, _pf, _pi, _pi]),
+    "qmcrt_diff_plain": (_i, [_vp, _vp]),
+    "qmcrt_diff_image": (_i, [_vp, _i, _pf, _pi, _pi]),
+    "qmcrt_diff_power": (_i, [_vp, _pd, _pd]),
+    "qmcrt_diff_create_suns": (_i, [_vp, _pf, _i, _f, ctypes.POINTER(_vp)]),
+    "qmcrt_diff_set_hit_records": (_i, [_vp, _i, ctypes.c_longlong]),
+    "qmcrt_diff_hit_records": (_i, [_vp, _pi, ctypes.POINTER(ctypes.c_longlong)]),
 }
 
 _lib = None

@@ -115,14 +115,15 @@ void batch_build_prefix(qmcrt_batch* b) {
   b->total_chunks = prefix.back();
 }
 
-cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out) {
+cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chunk_begin, long long chunk_end) {
   qm::TraceParams p{};
   p.grids = b->d_grids.as<qm::DevGrid>();
   p.receivers = b->d_receivers.as<qm::DevReceiver>();
   p.tasks = b->d_tasks.as<qm::DevTask>();
   p.facet_prefix = b->d_prefix.as<long long>();
   p.num_tasks = (int)b->tasks.size();
-  p.total_facets = b->total_chunks;
+  p.chunk_begin = chunk_begin;
+  p.total_facets = chunk_end < 0 ? b->total_chunks : std::min(chunk_end, b->total_chunks);
   p.light_begin = b->light_begin;
   p.light_end = b->light_end;
   p.power = b->d_power.as<double>();

@@ -59,7 +59,8 @@ namespace qrt {
 void batch_prepare(qmcrt_batch* b, cudaStream_t st);
 // Chunk prefix of the tasks for the current light range.
 void batch_build_prefix(qmcrt_batch* b);
-// One trace launch over all tasks; out as qm::launch_trace_*.
-cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out);
+// One trace launch over the tasks' warp chunks [chunk_begin, chunk_end)
+// (chunk_end < 0: to the last); out as qm::launch_trace_*.
+cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chunk_begin = 0, long long chunk_end = -1);
 
 }  // namespace qrt

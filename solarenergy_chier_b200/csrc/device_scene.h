@@ -79,12 +79,15 @@ struct TraceParams {
   const DevTask* tasks;
   const long long* facet_prefix;  // num_tasks + 1 prefix sums of warp chunks per task
   int num_tasks;
-  long long total_facets;         // total warp chunks of the launch
+  long long total_facets;         // end of the launch's warp chunks (chunks [chunk_begin, total_facets))
+  long long chunk_begin;          // first warp chunk of the launch (0: all)
   int light_begin, light_end;     // light indexes traced per facet
   int lights_q32, lights_r32;     // 32 / (light_end - light_begin) and 32 % it (set by the launcher)
   double* power;                  // FP64 per-slot power accumulators
   unsigned long long* diag;
-  // bilinear-deposit variant only: one word per warp iteration, bit i = lane i's ray hit the receiver
+  // bilinear-deposit and hit-bit variants: one word per warp iteration of the
+  // launch (chunk - chunk_begin), bit i = lane i's ray hit the receiver; may
+  // be NULL for the bilinear deposit
   uint32_t* hit_bits;
   // hit-record variant only
   int32_t* records;

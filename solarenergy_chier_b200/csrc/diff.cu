@@ -338,10 +338,11 @@ constexpr int kChunk = 32 * kChunkIters;
 __global__ void __launch_bounds__(256) diff_backward_kernel(BackwardParams p) {
   const int lane = threadIdx.x & 31;
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (warp >= p.total_chunks) return;
+  const long long chunk = p.chunk_begin + warp;
+  if (chunk >= p.total_chunks) return;
   const int nl = p.light_end - p.light_begin;
-  const int t = find_task(p.chunk_prefix, p.num_tasks, warp);
-  const int r0 = (int)(warp - __ldg(p.chunk_prefix + t)) * kChunk;
+  const int t = find_task(p.chunk_prefix, p.num_tasks, chunk);
+  const int r0 = (int)(chunk - __ldg(p.chunk_prefix + t)) * kChunk;
   const DevTask& T = p.tasks[t];
   const DiffTask& DT = p.dtasks[t];
   const DevReceiver& R = p.receivers[T.receiver];
@@ -430,11 +431,12 @@ cudaError_t launch_diff_prep(const PrepItem* items, int n, const DevTask* tasks,
 
 cudaError_t launch_diff_backward(const BackwardParams& params, cudaStream_t stream) {
   const long long nl = params.light_end - params.light_begin;
-  if (nl <= 0 || params.total_chunks <= 0) return cudaSuccess;
+  if (params.chunk_begin < 0) return cudaErrorInvalidValue;
+  if (nl <= 0 || params.total_chunks <= params.chunk_begin) return cudaSuccess;
   BackwardParams p = params;
   p.lights_q32 = (int)(32 / nl);
   p.lights_r32 = (int)(32 % nl);
-  const long long blocks = (p.total_chunks + 7) / 8;
+  const long long blocks = (p.total_chunks - p.chunk_begin + 7) / 8;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
   diff_backward_kernel<<<(unsigned)blocks, 256, 0, stream>>>(p);
   return cudaGetLastError();

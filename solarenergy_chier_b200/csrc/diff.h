@@ -33,10 +33,13 @@ struct BackwardParams {
   const DevReceiver* receivers;   // images hold P = G * dL/dF (the smoothed residual)
   const long long* chunk_prefix;  // as TraceParams::facet_prefix
   int num_tasks;
-  long long total_chunks;
+  long long total_chunks;         // end of the launch's chunks (chunks [chunk_begin, total_chunks))
+  long long chunk_begin;
   int light_begin, light_end;
   int lights_q32, lights_r32;
-  const uint32_t* hit_bits;       // written by the forward's bilinear-deposit launch
+  // one word per warp iteration of the launch (chunk - chunk_begin): the
+  // forward's bilinear-deposit launch, or a hit-bit launch over the same chunks
+  const uint32_t* hit_bits;
   double* grad;                   // kDiffParams per power slot
 };
 

@@ -334,7 +334,10 @@ __device__ __forceinline__ WalkStart window_start(const FacetWindow& win, int sl
 // Output of a launch: flux into the receiver images (nearest pixel, the
 // reference's deposit), per-ray outcome codes, or the differentiable
 // forward's bilinear deposit plus one hit bit per ray.
-enum TraceOut { kOutFlux = 0, kOutRecord = 1, kOutSplat = 2 };
+// Outputs: flux image (plain path), per-ray outcome codes, bilinear FP64
+// deposit + hit bits (differentiable forward), hit bits alone (the adjoint
+// recomputing its hit records).
+enum TraceOut { kOutFlux = 0, kOutRecord = 1, kOutSplat = 2, kOutBits = 3 };
 
 // Bilinear deposit of energy e at continuous pixel position (X, Y) (pixel c
 // spans [c, c+1), centres at c + 0.5): columns wrap around for a cylinder
@@ -378,9 +381,10 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
     r0 = p.record_facet_begin * nl + (int)warp * kChunk;
     r_end = p.record_facet_end * nl;
   } else {
-    if (warp >= p.total_facets) return;  // total_facets holds the number of chunks
-    t = find_task(p.facet_prefix, p.num_tasks, warp);
-    r0 = (int)(warp - __ldg(p.facet_prefix + t)) * kChunk;
+    const long long chunk = p.chunk_begin + warp;
+    if (chunk >= p.total_facets) return;  // total_facets holds the end chunk
+    t = find_task(p.facet_prefix, p.num_tasks, chunk);
+    r0 = (int)(chunk - __ldg(p.facet_prefix + t)) * kChunk;
     r_end = p.tasks[t].num_facets * nl;
   }
   // The task stays in global memory (L1-resident) and is read where used.
@@ -471,7 +475,9 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
             code = kMissed;
           } else {
             float e = qs::ray_energy(tt, rd, n, T.factor);
-            if (kOut == kOutSplat) {
+            if (kOut == kOutBits) {
+              code = 0;
+            } else if (kOut == kOutSplat) {
               splat_bilinear(R, qm_rn_mul(vv, (float)R.resolution.x), qm_rn_mul(uu, (float)R.resolution.y), e);
               power += (double)e;
               code = 0;
@@ -492,11 +498,11 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         }
       }
       if (kOut == kOutRecord) p.records[(size_t)(f - p.record_facet_begin) * nl + l] = code;
-      if (kOut == kOutSplat) hit = code >= 0;
+      if (kOut == kOutSplat || kOut == kOutBits) hit = code >= 0;
     }
-    if (kOut == kOutSplat) {
+    if (kOut == kOutSplat || kOut == kOutBits) {
       const unsigned bits = __ballot_sync(0xffffffffu, hit);
-      if (lane == 0) p.hit_bits[warp * kChunkIters + it] = bits;
+      if (lane == 0 && p.hit_bits) p.hit_bits[warp * kChunkIters + it] = bits;
     }
     f += q32;
     l += r32;
@@ -546,13 +552,15 @@ cudaError_t QM_SYM(launch_trace)(const TraceParams& params, int out, cudaStream_
   p.lights_r32 = (int)(32 % nl);
   const bool record = out == kOutRecord;
   const long long warps = record ? ((long long)(p.record_facet_end - p.record_facet_begin) * nl + kChunk - 1) / kChunk
-                                 : p.total_facets;
+                                 : p.total_facets - p.chunk_begin;
+  if (!record && p.chunk_begin < 0) return cudaErrorInvalidValue;
   if (warps <= 0) return cudaSuccess;
   const long long blocks = (warps + (threads / 32) - 1) / (threads / 32);
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
   switch (out) {
     case kOutRecord: trace_kernel<kOutRecord><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
     case kOutSplat: trace_kernel<kOutSplat><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
+    case kOutBits: trace_kernel<kOutBits><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
     default: trace_kernel<kOutFlux><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
   }
   return cudaGetLastError();

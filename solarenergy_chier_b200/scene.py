@@ -352,13 +352,32 @@ class Diff:
     (a, b) in radians; `forward()` returns the loss against the target flux,
     `backward()` its gradient, shape (num_heliostats, 4)."""
 
-    def __init__(self, scene: Scene, sigma_px: float = 2.0):
+    def __init__(self, scene: Scene, sigma_px: float = 2.0, suns=None):
+        """suns: None for the scene's own sun, else sun directions (n, 3): one
+        pair over all of them, parameters shared, receiver index k * R + r."""
         self._lib = load()
         self._scene = scene  # the scene must outlive the pair
         h = ctypes.c_void_p()
-        check(self._lib.qmcrt_diff_create(scene.handle, float(sigma_px), ctypes.byref(h)))
+        if suns is None:
+            check(self._lib.qmcrt_diff_create(scene.handle, float(sigma_px), ctypes.byref(h)))
+            self.num_suns = 1
+        else:
+            d = np.ascontiguousarray(np.asarray(suns, np.float32).reshape(-1, 3))
+            check(self._lib.qmcrt_diff_create_suns(scene.handle, _ptr(d, ctypes.c_float), d.shape[0],
+                                                   float(sigma_px), ctypes.byref(h)))
+            self.num_suns = d.shape[0]
         self._h = h
         self.num_heliostats = scene.num_heliostats
+
+    def set_hit_records(self, mode: int, segment_rays: int = 0) -> None:
+        """0 automatic, 1 checkpoint, 2 recompute (segment_rays per segment; 0 keeps it)."""
+        check(self._lib.qmcrt_diff_set_hit_records(self._h, int(mode), int(segment_rays)))
+
+    def hit_records(self) -> tuple[bool, int]:
+        """(recomputed, checkpoint bytes) of the last forward."""
+        r, n = ctypes.c_int(), ctypes.c_longlong()
+        check(self._lib.qmcrt_diff_hit_records(self._h, ctypes.byref(r), ctypes.byref(n)))
+        return bool(r.value), n.value
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
@@ -383,7 +402,11 @@ class Diff:
         check(self._lib.qmcrt_diff_set_params(self._h, pa, pn))
 
     def set_target(self, target: np.ndarray, receiver: int = 0) -> None:
+        w, h = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.qmcrt_diff_flux(self._h, receiver, None, ctypes.byref(w), ctypes.byref(h)))
         t = np.ascontiguousarray(np.asarray(target, np.float32))
+        if t.shape != (h.value, w.value):
+            raise ValueError(f"target shape {t.shape} != receiver image ({h.value}, {w.value})")
         check(self._lib.qmcrt_diff_set_target(self._h, receiver, _ptr(t, ctypes.c_float)))
 
     def set_light_range(self, begin: int, end: int) -> None:
@@ -405,6 +428,26 @@ class Diff:
         out = np.zeros((h.value, w.value), np.float32)
         check(self._lib.qmcrt_diff_flux(self._h, receiver, _ptr(out, ctypes.c_float), ctypes.byref(w), ctypes.byref(h)))
         return out
+
+    def plain(self, stream=None) -> None:
+        """Trace the current parameters with the plain tracer (nearest-pixel flux)."""
+        check(self._lib.qmcrt_diff_plain(self._h, _stream_handle(stream)))
+
+    def image(self, receiver: int = 0) -> np.ndarray:
+        """Unsmoothed flux of the last trace (forward: bilinear deposit; plain: binned)."""
+        w, h = ctypes.c_int(), ctypes.c_int()
+        check(self._lib.qmcrt_diff_image(self._h, receiver, None, ctypes.byref(w), ctypes.byref(h)))
+        out = np.zeros((h.value, w.value), np.float32)
+        check(self._lib.qmcrt_diff_image(self._h, receiver, _ptr(out, ctypes.c_float), ctypes.byref(w),
+                                         ctypes.byref(h)))
+        return out
+
+    def power(self) -> tuple[np.ndarray, float]:
+        """FP64 per-heliostat powers and total of the last trace."""
+        per = np.zeros(self.num_heliostats, np.float64)
+        total = ctypes.c_double()
+        check(self._lib.qmcrt_diff_power(self._h, _ptr(per, ctypes.c_double), ctypes.byref(total)))
+        return per, total.value
 
 
 def smooth_device(device_ptr: int, width: int, height: int, radius: int, ratio: float, stream=None) -> None:

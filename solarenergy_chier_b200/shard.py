@@ -95,7 +95,7 @@ def reduce_flux(images, per_heliostat, group=None, dst: int = 0):
     import torch.distributed as dist
 
     per = per_heliostat.to(torch.float64).reshape(-1).clone()
-    if dist.is_initialized() and dist.get_world_size(group) > 1:
+    if dist.is_initialized():
         for img in images:
             dist.reduce(img, dst, op=dist.ReduceOp.SUM, group=group)
         dist.all_reduce(per, op=dist.ReduceOp.SUM, group=group)

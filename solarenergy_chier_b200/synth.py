@@ -16,6 +16,15 @@ the direction of travel, -(cos e sin a, sin e, cos e cos a) for azimuth a
                 100-750 m over +-70 degrees, cylinder receiver r = 4 m,
                 h = 12 m at 115 m, 0.02 m micro-facets (300,664 per
                 heliostat), 20 m grid cells, 0.02 m receiver pixels (1257x600).
+  uneven_field  one of the batch's seeded fields of uneven size: 200-2500
+                square 6-12 m heliostats on radial-staggered rings sized to
+                the count, a rectangle (flat heliostats) or cylinder
+                (focus-flat 2x2 heliostats) receiver, 0.05 m micro-facets,
+                grid cells scaled to the heliostat size.
+  huge_field    10,000 flat 10x10 m heliostats on radial-staggered rings
+                150-1800 m over +-70 degrees, cylinder receiver r = 10 m,
+                h = 20 m at 200 m, 0.05 m micro-facets (40,000 per
+                heliostat), 20 m grid cells, 0.05 m receiver pixels.
 """
 from __future__ import annotations
 
@@ -165,3 +174,68 @@ def large_field(out_dir, seed: int = 0, num_heliostats: int = 624, helio_pixel: 
               "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
     block = ["gap\t0.000000\t0.000000", f"matrix\t{rows}\t{cols}", "surface_property -1 -1 -1 -1 -1 -1"]
     return _write(out_dir, "large", recv, grid, block, pos, (12.84, 0.1, 9.45), config)
+
+
+def uneven_field(out_dir, index: int, seed: int = 0, helio_pixel: float = 0.05, receiver_pixel: float = 0.05,
+                 groups: int = 128, per_group: int = 2048) -> SceneFiles:
+    """Field `index` of the batch's uneven fields (seeded by seed and index).
+
+    Even indexes: flat square heliostats and a vertical rectangle receiver
+    facing the field; odd indexes: focus-flat 2x2 heliostats (focal length =
+    slant range) and a cylinder receiver.  Heliostat count uniform in
+    [200, 2500], side uniform in [6, 12] m, rings from 60 m + 3 sides out to
+    the radius that leaves about (3 sides)^2 of ground per heliostat over
+    +-70 degrees.
+    """
+    rng = np.random.default_rng([seed, index, 0x5EED])
+    n = int(rng.integers(200, 2501))
+    side = float(rng.uniform(6.0, 12.0))
+    r_min = 60.0 + 3.0 * side
+    span = math.radians(140.0)
+    r_max = math.sqrt(r_min ** 2 + n * (3.0 * side) ** 2 / (0.5 * span))
+    xz = radial_staggered(n, r_min, r_max, 70.0, int(rng.integers(1 << 30)))
+    pos = np.stack([xz[:, 0], np.full(n, 0.5 * side + 0.5), xz[:, 1]], axis=1)
+    tower = 40.0 + 0.08 * r_max
+    cylinder = index % 2 == 1
+    if cylinder:
+        r, h = float(rng.uniform(3.0, 8.0)), float(rng.uniform(8.0, 16.0))
+        recv = ["Recv\t1", f"pos\t\t0.000000\t{_fmt(tower)}\t0.000000", f"size\t{_fmt(r)}\t{_fmt(h)}\t0.000000",
+                "norm\t0.000000\t1.000000\t0.000000", "face\t0", "end"]
+        block = ["gap\t0.000000\t0.000000", "matrix\t2\t2", "surface_property -1 -1 -1 -1 -1 -1"]
+    else:
+        w, h = float(rng.uniform(8.0, 14.0)), float(rng.uniform(6.0, 10.0))
+        recv = ["Recv\t0", f"pos\t\t0.000000\t{_fmt(tower)}\t0.000000", f"size\t{_fmt(w)}\t{_fmt(h)}\t0.100000",
+                "norm\t0.000000\t0.000000\t1.000000", "face\t0", "end"]
+        block = ["gap\t0.000000\t0.000000", "matrix\t1\t1"]
+    cell = float(max(10.0, round(1.6 * side)))
+    margin = cell
+    x0 = float(np.floor(pos[:, 0].min() - margin))
+    z0 = float(np.floor(pos[:, 2].min() - margin))
+    grid = {"pos": [x0, 0.0, z0], "size": [float(np.ceil(pos[:, 0].max() + margin - x0)), cell,
+                                            float(np.ceil(pos[:, 2].max() + margin - z0))],
+            "inter": [cell, cell, cell], "helio_type": 1 if cylinder else 0}
+    config = {"sun_dir": sun_direction(float(rng.uniform(120.0, 240.0)), float(rng.uniform(25.0, 75.0))),
+              "dni": 1000.0, "csr": 0.1, "num_of_sunshape_groups": groups, "num_per_sunshape_group": per_group,
+              "inverse_transform_sampling_groups": 1024, "receiver_pixel_length": receiver_pixel,
+              "helio_disturb_std": 0.002, "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
+    return _write(out_dir, f"uneven{index:02d}", recv, grid, block, pos, (side, 0.1, side), config)
+
+
+def huge_field(out_dir, seed: int = 0, num_heliostats: int = 10_000, helio_pixel: float = 0.05,
+               receiver_pixel: float = 0.05, groups: int = 128, per_group: int = 2048) -> SceneFiles:
+    """The large batched-adjoint field: flat 10x10 m heliostats, cylinder receiver."""
+    xz = radial_staggered(num_heliostats, 150.0, 1800.0, 70.0, seed)
+    pos = np.stack([xz[:, 0], np.full(len(xz), 5.5), xz[:, 1]], axis=1)
+    recv = ["Recv\t1", "pos\t\t0.000000\t200.000000\t0.000000", "size\t10.000000\t20.000000\t0.000000",
+            "norm\t0.000000\t1.000000\t0.000000", "face\t0", "end"]
+    x0 = float(np.floor(pos[:, 0].min() - 20.0))
+    z0 = float(np.floor(pos[:, 2].min() - 20.0))
+    grid = {"pos": [x0, 0.0, z0], "size": [float(np.ceil(pos[:, 0].max() + 20.0 - x0)), 20.0,
+                                            float(np.ceil(pos[:, 2].max() + 20.0 - z0))],
+            "inter": [20.0, 20.0, 20.0], "helio_type": 0}
+    config = {"sun_dir": sun_direction(180.0, 60.0), "dni": 1000.0, "csr": 0.1, "num_of_sunshape_groups": groups,
+              "num_per_sunshape_group": per_group, "inverse_transform_sampling_groups": 1024,
+              "receiver_pixel_length": receiver_pixel, "helio_disturb_std": 0.002,
+              "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
+    return _write(out_dir, "huge", recv, grid, ["gap\t0.000000\t0.000000", "matrix\t1\t1"], pos,
+                  (10.0, 0.1, 10.0), config)

@@ -108,3 +108,24 @@ def test_autotune_and_errors(fields):
         q.Batch(scenes, [(2, SUNS[0])])
     with pytest.raises(q.QmcrtError):
         q.Batch(scenes, [(0, [0.0, 0.0, 0.0])])
+
+
+def test_uneven_fields_batch_equals_plain(tmp_path):
+    """Two of the batch benchmark's uneven fields (a rectangle receiver with
+    flat heliostats, a cylinder with focus-flat ones), coarse facets, at
+    their own suns and at a shared one, in one batch with mismatched sizes."""
+    files = [synth.uneven_field(tmp_path, k, seed=3, helio_pixel=0.75, groups=4, per_group=128) for k in (0, 1)]
+    scenes = [q.Scene(f.scene, f.config, device=0, seed=11) for f in files]
+    own = [np.array(s.info.sun_dir[:], np.float32) for s in scenes]
+    inst = [(0, own[0]), (1, own[1]), (1, SUNS[1]), (0, SUNS[2])]
+    b = q.Batch(scenes, inst)
+    b.set_math_mode(1)
+    b.trace()
+    for k, (si, sun) in enumerate(inst):
+        _, img, per, total = plain_reference(files[si], sun, 1)
+        assert total > 0, f"instance {k}: no energy"
+        got = b.image(k).astype(np.float64)
+        assert np.abs(got - img).sum() <= 1e-5 * img.sum(), f"instance {k}"
+        gper, gtotal = b.power(k)
+        assert abs(gtotal - total) <= 1e-9 * total
+        assert np.allclose(gper, per, rtol=1e-9, atol=0)

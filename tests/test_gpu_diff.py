@@ -90,3 +90,117 @@ def test_adjoint_matches_central_differences(field):
             if rel > bar:
                 failures.append(f"{name} {cols}: {rel:.3e} > {bar}")
     assert not failures, failures
+
+
+def test_aim_optimisation_checked_by_the_plain_tracer(field):
+    """Adam on the aim offsets from a perturbed start back toward the flux
+    of the unperturbed field; every step re-traced by the plain tracer.
+    Bars: both losses fall by more than half; the forward's and the plain
+    tracer's FP64 powers agree to 1e-9 every step (the same hits); the
+    plain tracer's smoothed flux is within 5 % L1 of the splatted flux."""
+    from solarenergy_chier_b200 import aim
+
+    s, d = make(field)
+    d.set_light_range(0, 64)
+    H = s.num_heliostats
+    d.set_params()
+    d.set_target(np.zeros((s.receiver(0)["height"], s.receiver(0)["width"]), np.float32))
+    d.forward()
+    target = d.flux(0)
+    d.set_target(target)
+    rng = np.random.default_rng(3)
+    res = aim.optimise_aim(d, target, steps=25, lr_aim=0.05, aim0=rng.uniform(-0.5, 0.5, (H, 2)), check=True)
+    h = res.history
+    assert h[-1]["loss"] < 0.5 * h[0]["loss"]
+    assert h[-1]["plain_loss"] < 0.5 * h[0]["plain_loss"]
+    for r in h:
+        assert abs(r["power"] - r["plain_power"]) <= 1e-9 * r["plain_power"], r
+        assert r["plain_vs_splat_l1"] <= 0.05, r
+    assert np.all(np.abs(res.aim) <= 1.0)
+
+
+def test_plain_trace_keeps_the_adjoint_valid(field):
+    s, d = make(field)
+    d.set_light_range(0, 32)
+    H = s.num_heliostats
+    rng = np.random.default_rng(4)
+    d.set_params(rng.uniform(-0.3, 0.3, (H, 2)), rng.uniform(-3e-4, 3e-4, (H, 2)))
+    d.set_target(np.zeros((s.receiver(0)["height"], s.receiver(0)["width"]), np.float32))
+    d.forward()
+    g0 = d.backward()
+    d.forward()
+    d.plain()
+    np.testing.assert_allclose(d.backward(), g0, rtol=1e-12, atol=1e-12 * np.abs(g0).max())
+
+
+def test_recomputed_hit_records_give_the_checkpointed_gradient(field):
+    """The adjoint with hit records recomputed segment by segment (a hit-bit
+    trace before each adjoint launch) equals the one with the forward's
+    checkpointed records, up to the order of the FP64 gradient atomics."""
+    s, d = make(field)
+    d.set_light_range(0, 48)
+    H = s.num_heliostats
+    rng = np.random.default_rng(6)
+    d.set_params(rng.uniform(-0.3, 0.3, (H, 2)), rng.uniform(-3e-4, 3e-4, (H, 2)))
+    d.set_target(np.zeros((s.receiver(0)["height"], s.receiver(0)["width"]), np.float32))
+    d.set_hit_records(1)
+    l1 = d.forward()
+    assert d.hit_records()[0] is False and d.hit_records()[1] > 0
+    g1 = d.backward()
+    for seg in (256 * 7, 1 << 16, 0):
+        d.set_hit_records(2, seg)
+        l2 = d.forward()
+        assert d.hit_records() == (True, 0)
+        g2 = d.backward()
+        assert l2 == pytest.approx(l1, rel=1e-12)
+        np.testing.assert_allclose(g2, g1, rtol=1e-9, atol=1e-12 * np.abs(g1).max())
+    d.set_hit_records(0)
+    d.forward()
+    assert d.hit_records()[0] is False  # a small field: checkpointing fits
+    with pytest.raises(q.QmcrtError):
+        d.set_hit_records(3)
+
+
+def test_several_suns_in_one_pair(field):
+    """One pair over two suns equals the sum of two one-sun pairs: loss,
+    gradient (parameters shared by the suns), powers; receiver k = sun k."""
+    s = q.Scene(field.scene, field.config, device=0, seed=5)
+    suns = np.array([[0.0, -0.866, -0.5], [0.35, -0.75, 0.56]], np.float32)
+    H = s.num_heliostats
+    rng = np.random.default_rng(9)
+    aim, nrm = rng.uniform(-0.3, 0.3, (H, 2)), rng.uniform(-3e-4, 3e-4, (H, 2))
+    shape = (s.receiver(0)["height"], s.receiver(0)["width"])
+    targets = [np.full(shape, 50.0 * (k + 1), np.float32) for k in range(2)]
+    both = q.Diff(s, 2.0, suns=suns)
+    assert both.num_suns == 2
+    both.set_light_range(0, 32)
+    both.set_params(aim, nrm)
+    for k in range(2):
+        both.set_target(targets[k], receiver=k)
+    loss = both.forward()
+    grad = both.backward()
+    per, total = both.power()
+    want_loss, want_grad, want_per = 0.0, np.zeros((H, 4)), np.zeros(H)
+    for k in range(2):
+        one = q.Diff(s, 2.0, suns=suns[k:k + 1])
+        one.set_light_range(0, 32)
+        one.set_params(aim, nrm)
+        one.set_target(targets[k])
+        want_loss += one.forward()
+        want_grad += one.backward()
+        want_per += one.power()[0]
+        np.testing.assert_allclose(both.flux(k), one.flux(0), rtol=1e-5, atol=1e-6 * one.flux(0).max())
+        one.close()
+    assert loss == pytest.approx(want_loss, rel=1e-6)
+    np.testing.assert_allclose(grad, want_grad, rtol=1e-6, atol=1e-9 * np.abs(want_grad).max())
+    np.testing.assert_allclose(per, want_per, rtol=1e-12)
+    assert total == pytest.approx(want_per.sum(), rel=1e-12)
+    with pytest.raises(q.QmcrtError):
+        both.flux(2)
+    # one sun given explicitly equals the scene's own sun
+    own = q.Diff(s, 2.0, suns=np.array(s.info.sun_dir[:], np.float32)[None])
+    ref = q.Diff(s, 2.0)
+    for x in (own, ref):
+        x.set_light_range(0, 16)
+        x.set_target(targets[0])
+    assert own.forward() == pytest.approx(ref.forward(), rel=1e-12)

@@ -357,9 +357,11 @@ def test_sharded_trace_one_rank_equals_plain(small):
         s.trace(ids)  # the one-rank share of an 8-light trace
         images, per, total = shard.reduce_flux([shard.device_image_tensor(s, 0)],
                                                torch.from_numpy(s.power()[0]).cuda())
-        assert np.array_equal(images[0].cpu().numpy(), want_img)
-        assert np.array_equal(per.cpu().numpy(), want_per)
-        assert total == want_total
+        # two traces of the same rays: equal up to the order of the atomics
+        got = images[0].cpu().numpy().astype(np.float64)
+        assert np.abs(got - want_img).sum() <= 1e-5 * want_img.sum()
+        np.testing.assert_allclose(per.cpu().numpy(), want_per, rtol=1e-12)
+        assert total == pytest.approx(want_total, rel=1e-12)
         small.reset()
         st.trace(ids)
         images, per, total = st.reduce()

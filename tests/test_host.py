@@ -327,3 +327,20 @@ def test_pipeline_executable_rejects_bad_arguments(tmp_path):
     r = subprocess.run([str(exe), "-c", str(tmp_path / "x.txt")], capture_output=True, text=True)
     assert r.returncode != 0
     assert "suffix" in r.stderr
+
+
+def test_uneven_fields_load_with_the_documented_shapes(tmp_path):
+    counts, types = [], []
+    for k in range(16):
+        f = synth.uneven_field(tmp_path, k, seed=0, helio_pixel=1.0)
+        s = q.Scene(f.scene, f.config, device=-1)
+        assert 200 <= s.num_heliostats <= 2500
+        side = s.heliostat(0)["size"][0]
+        assert 6.0 <= side <= 12.0
+        assert s.receiver(0)["type"] == k % 2
+        counts.append(s.num_heliostats)
+        types.append(s.receiver(0)["type"])
+    assert len(set(counts)) > 8 and set(types) == {0, 1}
+    # seeded: the same index and seed write the same scene
+    a = synth.uneven_field(tmp_path / "a", 3, seed=0).scene.read_text()
+    assert a == synth.uneven_field(tmp_path / "b", 3, seed=0).scene.read_text()

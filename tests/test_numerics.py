@@ -30,3 +30,39 @@ def test_float_comparisons_with_double_epsilon():
             assert np.array_equal(d > -1e-5, x >= -eps32)
             assert np.array_equal(d >= -1e-5, x >= -eps32)
             assert np.array_equal(d < -1e-5, x < -eps32)
+
+
+def test_aim_smoothing_and_adam():
+    """Host pieces of the aim optimisation (solarenergy_chier_b200/aim.py):
+    the FP64 smoothing equals a direct double loop of the pair's separable
+    Gaussian (rows wrapping on a cylinder, columns zero outside), and Adam's
+    first step moves every coordinate by lr against the gradient's sign."""
+    from solarenergy_chier_b200 import aim
+
+    rng = np.random.default_rng(2)
+    img = rng.random((9, 13))
+    w = aim.gaussian_weights(1.5).astype(np.float64)
+    r = len(w) - 1
+    for wrap in (True, False):
+        tmp = np.zeros_like(img)
+        for y in range(9):
+            for x in range(13):
+                for k in range(-r, r + 1):
+                    c = x + k
+                    if wrap:
+                        c %= 13
+                    if 0 <= c < 13:
+                        tmp[y, x] += w[abs(k)] * img[y, c]
+        want = np.zeros_like(img)
+        for y in range(9):
+            for x in range(13):
+                for k in range(-r, r + 1):
+                    if 0 <= y + k < 9:
+                        want[y, x] += w[abs(k)] * tmp[y + k, x]
+        np.testing.assert_allclose(aim.gaussian_smooth(img, 1.5, wrap), want, rtol=1e-13)
+    opt = aim.Adam((3,), lr=0.1)
+    x = opt.step(np.zeros(3), np.array([2.0, -5.0, 1e-3]))
+    np.testing.assert_allclose(x, [-0.1, 0.1, -0.1], rtol=1e-4)
+    t = aim.smooth_target(np.outer(np.hanning(40), np.hanning(60)), seed=1)
+    lit = t > 0
+    assert t.max() / t[lit].mean() <= 2.0
