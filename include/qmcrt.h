@@ -49,6 +49,11 @@ int qmcrt_scene_load(const char* scene_path, const char* config_path, int device
                      qmcrt_scene** out);
 /* Replaces SolarScene::clear (Scene/SolarScene.cpp:31-46). */
 void qmcrt_scene_free(qmcrt_scene* scene);
+/* Replaces SceneConfiguration::loadConfiguration's parse alone
+ * (Scene/SceneConfiguration.cpp:39-69): reads and checks a configuration
+ * file; fields receives how many of the 10 keys it sets.  A missing or
+ * malformed file is QMCRT_ERR_IO (the reference throws). */
+int qmcrt_config_check(const char* config_path, int* fields);
 
 /* New sun direction (direction of travel, as the configuration's "sun_dir").
  * Replaces reloading the configuration and re-running the sun-dependent half

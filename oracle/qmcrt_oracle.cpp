@@ -269,13 +269,18 @@ void helio_orient(Helio<T>& h, V<T> focus, V<T> sun) {
 }
 
 // Sub-heliostat lengths and micro-facet lattice (RectangleHelio.cu:84-104,
-// FocusFlatRectangleHelio.cu:68-82).
+// FocusFlatRectangleHelio.cu:68-82).  The lattice counts are evaluated in
+// float in both precisions: they decide which micro-facets exist (4 m /
+// 0.05 m is 80 facets in float, 79 in double), and the FP64 oracle traces
+// the same facets as the float one, only in double.
 template <class T>
 void helio_lattice(Helio<T>& h) {
   h.len_x = (h.size.z - h.gap_y * T(h.rows - 1)) / T(h.rows);
   h.len_y = (h.size.x - h.gap_x * T(h.cols - 1)) / T(h.cols);
-  h.sub_rows = int(h.len_x / h.pixel_length);
-  h.sub_cols = int(h.len_y / h.pixel_length);
+  const float lx = ((float)h.size.z - (float)h.gap_y * float(h.rows - 1)) / float(h.rows);
+  const float ly = ((float)h.size.x - (float)h.gap_x * float(h.cols - 1)) / float(h.cols);
+  h.sub_rows = int(lx / (float)h.pixel_length);
+  h.sub_cols = int(ly / (float)h.pixel_length);
   h.n_facets = h.rows * h.cols * h.sub_rows * h.sub_cols;
 }
 

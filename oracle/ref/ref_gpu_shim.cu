@@ -5,7 +5,9 @@
 // oracle/build_ref.py into oracle/_ref/libref_gpu.so with the real CUDA
 // runtime and cuRAND).  bench.py uses it to time the reference's tracer on
 // the same B200: QuasiMonteCarloRayTracer::rayTracing per heliostat, end to
-// end (B1), and the map_raytracing launch alone (B2).
+// end (B1), and the map_raytracing launch alone (B2); tests/test_gpu_reference.py
+// (through oracle/ref_gpu_parity.py) injects sample pools and facet offsets
+// and compares the reference kernel's flux maps with this tracer's.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -166,6 +168,78 @@ int refgpu_lights_per_group() { return SolarScene::GetInstance()->getSunray()->g
 int refgpu_pool_size() {
   Sunray* sun = SolarScene::GetInstance()->getSunray();
   return sun->getNumOfSunshapeGroups() * sun->getNumOfSunshapeLightsPerGroup();
+}
+
+// Replaces the sun's sample pools after processScene, as the reference's
+// own tests do (Sunray::CClear, then setDeviceSampleLights /
+// setDevicePerturbation with new device arrays; receiverIntersectUtil.cpp:8-33).
+int refgpu_set_pools(const float* dirs, const float* perturbations, int n) {
+  Sunray* sun = SolarScene::GetInstance()->getSunray();
+  if (n != sun->getNumOfSunshapeGroups() * sun->getNumOfSunshapeLightsPerGroup()) {
+    g_err = "pool size differs from groups x lights per group";
+    return -2;
+  }
+  sun->CClear();
+  float3 *d_dirs = nullptr, *d_pert = nullptr;
+  if (cudaMalloc(&d_dirs, sizeof(float3) * n) != cudaSuccess || cudaMalloc(&d_pert, sizeof(float3) * n) != cudaSuccess) {
+    g_err = "cudaMalloc failed";
+    return -4;
+  }
+  cudaMemcpy(d_dirs, dirs, sizeof(float3) * n, cudaMemcpyHostToDevice);
+  cudaMemcpy(d_pert, perturbations, sizeof(float3) * n, cudaMemcpyHostToDevice);
+  sun->setDeviceSampleLights(d_dirs);
+  sun->setDevicePerturbation(d_pert);
+  return cudaGetLastError() == cudaSuccess ? 0 : -4;
+}
+
+// The reference's tracing launch for one heliostat with the given facet
+// offsets (num_facets + 1 entries: the launch reads entry f + 1 for facet f)
+// in place of its cuRAND ones, accumulating into its receiver image: its
+// vertex table, micro-facets and launcher unchanged.
+int refgpu_trace_with_offsets(int id, const int* offsets, int n_offsets) {
+  try {
+    SolarScene* s = SolarScene::GetInstance();
+    QuasiMonteCarloRayTracer tracer;
+    Sunray* sun = s->getSunray();
+    Heliostat* h = s->getHeliostats()[id];
+    Grid* grid = s->getGrids()[h->getBelongingGridId()];
+    Receiver* recv = s->getReceivers()[grid->getBelongingReceiverIndex()];
+    float3* verts = nullptr;
+    tracer.setFlatRectangleHeliostatVertexs(verts, s->getHeliostats(), grid->getStartHeliostatIndex(),
+                                            grid->getStartHeliostatIndex() + grid->getNumberOfHeliostats());
+    SunrayArgument sa = tracer.generateSunrayArgument(sun);
+    HeliostatArgument ha = tracer.generateHeliostatArgument(s, id);
+    if (n_offsets != ha.numberOfMicroHeliostats + 1) {
+      cudaFree(verts);
+      ha.CClear();
+      g_err = "offsets must hold num_facets + 1 entries";
+      return -2;
+    }
+    cudaFree(ha.d_microHelio_groups);
+    ha.d_microHelio_groups = nullptr;
+    cudaMalloc(&ha.d_microHelio_groups, sizeof(int) * n_offsets);
+    cudaMemcpy(ha.d_microHelio_groups, offsets, sizeof(int) * n_offsets, cudaMemcpyHostToDevice);
+    float ratio = h->getPixelLength() / recv->getPixelLength();
+    float factor = sun->getDNI() * ratio * ratio * sun->getReflectiveRate() / float(sun->getNumOfSunshapeLightsPerGroup());
+    if (recv->getType() == 0)
+      RectangleReceiverRectangleGridRayTracing(sa, dynamic_cast<RectangleReceiver*>(recv),
+                                               dynamic_cast<RectangleGrid*>(grid), ha, verts, factor);
+    else
+      CylinderReceiverRectangleGridRayTracing(sa, dynamic_cast<CylinderReceiver*>(recv),
+                                              dynamic_cast<RectangleGrid*>(grid), ha, verts, factor);
+    cudaDeviceSynchronize();
+    cudaFree(verts);
+    ha.CClear();
+    return cudaGetLastError() == cudaSuccess ? 0 : -4;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+int refgpu_clear_image(int r) {
+  SolarScene::GetInstance()->getReceivers()[r]->Cclean_image_content();
+  return cudaGetLastError() == cudaSuccess ? 0 : -4;
 }
 
 // Receiver image read-back (float, rows x cols).

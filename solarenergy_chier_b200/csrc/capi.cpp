@@ -497,6 +497,17 @@ int qmcrt_scene_load(const char* scene_path, const char* config_path, int device
 
 void qmcrt_scene_free(qmcrt_scene* s) { delete s; }
 
+int qmcrt_config_check(const char* config_path, int* fields) {
+  return guarded([&] {
+    if (!config_path) invalid("configuration path is NULL");
+    qm::SceneConfig cfg;
+    std::string err;
+    const int n = qm::read_config_file(config_path, cfg, err);
+    if (n < 0) throw ApiError(QMCRT_ERR_IO, err);
+    if (fields) *fields = n;
+  });
+}
+
 int qmcrt_scene_get_info(const qmcrt_scene* s, qmcrt_scene_info* info) {
   return guarded([&] {
     if (!s || !info) invalid("scene or info is NULL");

@@ -73,6 +73,16 @@ enum RayCode : int32_t { kShadowed = -1, kBlocked = -2, kMissed = -3, kNotTraced
 // Diagnostic counters (unsigned long long each).
 enum DiagSlot { kDiagClamped = 0, kDiagDdaCap = 1, kDiagSlots = 4 };
 
+// Warp chunk: every launch over tasks hands each warp kChunkIters x 32
+// consecutive rays of one task (trace_kernel, diff_backward_kernel; hit bits
+// are one word per chunk iteration).  Larger chunks amortise the per-chunk
+// work (task lookup, facet window fill, power reduction) over more rays.
+#ifndef QM_CHUNK_ITERS
+#define QM_CHUNK_ITERS 8
+#endif
+constexpr int kChunkIters = QM_CHUNK_ITERS;
+constexpr int kChunk = 32 * kChunkIters;
+
 struct TraceParams {
   const DevGrid* grids;
   const DevReceiver* receivers;

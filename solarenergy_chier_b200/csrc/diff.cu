@@ -332,8 +332,6 @@ __device__ __forceinline__ void ray_adjoint(const DevTask& T, const DiffTask& DT
   }
 }
 
-constexpr int kChunkIters = 8;  // as the trace kernel: 256 rays per warp chunk
-constexpr int kChunk = 32 * kChunkIters;
 
 __global__ void __launch_bounds__(256) diff_backward_kernel(BackwardParams p) {
   const int lane = threadIdx.x & 31;

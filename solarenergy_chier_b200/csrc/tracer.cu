@@ -276,8 +276,6 @@ __device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, flo
 // facet past its end (once per chunk for nl >= 9).  Per-ray work then reads
 // the window instead of re-deriving the facet, and holds no facet state in
 // registers across the grid walks.
-constexpr int kChunkIters = 8;
-constexpr int kChunk = 32 * kChunkIters;
 #ifndef QM_TRACE_THREADS
 #define QM_TRACE_THREADS 256
 #endif

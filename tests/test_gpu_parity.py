@@ -370,3 +370,19 @@ def test_sharded_trace_one_rank_equals_plain(small):
     finally:
         dist.destroy_process_group()
         small.reset()
+
+
+def test_cpp_facade_traces_like_the_python_binding(tmp_path, cuda_device):
+    """A host program written against the reference's entry points
+    (tests/facade_main.cpp over include/qmcrt_facade.hpp) traces the task
+    file's heliostats like the binding does with the same seed."""
+    from tests.test_host import build_facade_program, run_facade
+
+    files = synth.small_field(tmp_path, seed=1, helio_pixel=0.1)
+    res = run_facade(build_facade_program(tmp_path), files, tmp_path, 0)
+    s = q.Scene(files.scene, files.config, device=0, seed=0)
+    s.trace(list(range(s.num_heliostats)))
+    want = float(s.image(0).astype(np.float64).sum())
+    assert want > 0
+    assert float(res["image_sum"]) == pytest.approx(want, rel=1e-5)
+    assert (tmp_path / "facade_after_smooth.txt").exists() and float(res["saved_max"]) > 0

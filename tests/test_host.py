@@ -344,3 +344,32 @@ def test_uneven_fields_load_with_the_documented_shapes(tmp_path):
     # seeded: the same index and seed write the same scene
     a = synth.uneven_field(tmp_path / "a", 3, seed=0).scene.read_text()
     assert a == synth.uneven_field(tmp_path / "b", 3, seed=0).scene.read_text()
+
+
+def build_facade_program(tmp_path) -> Path:
+    """tests/facade_main.cpp compiled with g++ against include/qmcrt_facade.hpp, linked with libqmcrt.so."""
+    import subprocess
+
+    exe = tmp_path / "facade_main"
+    lib_dir = q.LIB_PATH.parent
+    r = subprocess.run(["g++", "-std=c++17", "-O1", f"-I{ROOT / 'include'}", str(ROOT / "tests" / "facade_main.cpp"),
+                        f"-L{lib_dir}", "-lqmcrt", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def run_facade(exe, files, out_dir, device: int) -> dict:
+    import subprocess
+
+    r = subprocess.run([str(exe), str(files.scene), str(files.config), str(files.tasks), str(out_dir), str(device)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    return dict(kv.split("=") for kv in r.stdout.split())
+
+
+def test_cpp_facade_with_the_reference_names_host_only(tmp_path):
+    files = synth.small_field(tmp_path, seed=1, helio_pixel=0.5)
+    res = run_facade(build_facade_program(tmp_path), files, tmp_path, -1)
+    assert res["fields"] == "10" and res["heliostats"] == "50"
+    assert res["tasks_ok"] == "1" and res["tasks"] == "50" and res["receivers"] == "1"
