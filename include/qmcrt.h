@@ -156,15 +156,19 @@ int qmcrt_power_clear(qmcrt_scene* scene);
  * [1] grid walks stopped by the step bound, [2..3] reserved. */
 int qmcrt_diagnostics(qmcrt_scene* scene, unsigned long long* out4);
 
-/* Debug: per heliostat, 1 when the tracer skips its shadow walks for the
- * current sun and pool because no other heliostat can shadow any of its rays
- * (a conservative capsule test around the sun-shape cone; no reference
- * counterpart -- the reference walks every ray). */
+/* Debug: per heliostat, the shadow-walk code for the current sun and pool:
+ * 1 when the tracer skips its shadow walks because no other heliostat can
+ * shadow any of its rays (a conservative capsule test around the sun-shape
+ * cone; no reference counterpart -- the reference walks every ray), k + 1
+ * when only k (<= 6) listed heliostats can (a ray whose path meets none of
+ * their padded boxes skips its walk), 0 when every ray walks. */
 int qmcrt_debug_shadow_free(qmcrt_scene* scene, int* flags);
 /* Debug: per sub-heliostat of a grid (grid-local ids, as qmcrt_grid_vertices),
- * 1 when the block walks of its facets are skipped because no other
- * heliostat can block a ray reflected from it (same kind of test around its
- * reflected cone). */
+ * the block-walk code of its facets for the current sun and pools: 1 when
+ * the walks are skipped because no other heliostat can block a ray
+ * reflected from it (same kind of test around its reflected cone), k + 1
+ * when only k (<= 6) listed heliostats can (a ray whose path meets none of
+ * their padded boxes skips its walk), 0 when every ray walks. */
 int qmcrt_debug_block_free(qmcrt_scene* scene, int grid, int* flags);
 
 /* Per-ray outcome for facets [facet_begin, facet_end) x lights [light_begin,

@@ -151,6 +151,7 @@ void build_device_scene(qmcrt_scene* s) {
     upload(gb->subv, subv);
     // block-free flags start cleared (no skipping) until the pools exist
     upload(gb->sub_free, std::vector<int>(std::max(g.num_subheliostats, 1), 0));
+    upload(gb->sub_cand, std::vector<int>((size_t)std::max(g.num_subheliostats, 1) * qm::kMaxCandidates, -1));
     DevGrid dg;
     dg.pos = g.pos;
     dg.interval = g.interval;
@@ -162,6 +163,7 @@ void build_device_scene(qmcrt_scene* s) {
     dg.hsub = gb->hsub.as<int4>();
     dg.subv = gb->subv.as<float4>();
     dg.sub_free = gb->sub_free.as<int>();
+    dg.sub_cand = gb->sub_cand.as<int>();
     s->grids.push_back(dg);
     s->grid_bufs.push_back(std::move(gb));
   }
@@ -290,7 +292,7 @@ void update_shadow_flags(qmcrt_scene* s, bool pools_changed) {
   sun_cone(sun, s->sun_shape_tan, axis, tan_world);
   qm::WalkFlagParams p{};
   upload(s->d_flag_tasks, s->templates);
-  s->d_flag_out.alloc(std::max<size_t>(s->templates.size(), 1) * sizeof(int));
+  s->d_flag_out.alloc(std::max<size_t>(s->templates.size(), 1) * (1 + qm::kMaxCandidates) * sizeof(int));
   p.tasks = s->d_flag_tasks.as<DevTask>();
   p.n = (int)s->templates.size();
   p.grids = s->d_grids.as<DevGrid>();
@@ -298,13 +300,19 @@ void update_shadow_flags(qmcrt_scene* s, bool pools_changed) {
   p.sun_tan = tan_world;
   p.sun_dir = sun;
   p.block_theta = tan_world < 0.0f || s->slope_angle < 0.0f ? -1.0f : std::atan(tan_world) + 2.0f * s->slope_angle;
+  const size_t nt = s->templates.size();
   p.shadow_out = s->d_flag_out.as<int>();
+  p.shadow_cand_out = s->d_flag_out.as<int>() + nt;
   cuda_check(qm::launch_walk_flags(p, 0), "walk flags");
-  std::vector<int> flags(s->templates.size());
+  std::vector<int> flags(nt * (1 + qm::kMaxCandidates));
   if (!flags.empty())
     cuda_check(cudaMemcpy(flags.data(), s->d_flag_out.p, flags.size() * sizeof(int), cudaMemcpyDeviceToHost),
                "walk flags");
-  for (size_t i = 0; i < flags.size(); ++i) s->templates[i].shadow_free = flags[i];
+  for (size_t i = 0; i < nt; ++i) {
+    s->templates[i].shadow_free = flags[i];
+    for (int k = 0; k < qm::kMaxCandidates; ++k)
+      s->templates[i].shadow_cand[k] = flags[nt + i * qm::kMaxCandidates + k];
+  }
   s->flags_valid = true;
   s->flags_sun = sun;
   s->flags_tan = s->sun_shape_tan;

@@ -9,6 +9,10 @@ namespace qm {
 
 // One RectangleGrid (Scene/DataStructure/Grid/RectangleGrid.cuh:13-52) in
 // traversal form.
+// Candidate heliostats kept per sub-heliostat (DevGrid::sub_cand) and per
+// task (DevTask::shadow_cand) for the walk pre-tests.
+constexpr int kMaxCandidates = 6;
+
 struct DevGrid {
   float3 pos;
   float3 interval;
@@ -20,7 +24,12 @@ struct DevGrid {
                         // for k = lattice x, normal, lattice z, then (x0, 1/px, z0, 1/pz)
   const int4* hsub;     // (first sub-heliostat id, count, lattice rows, lattice columns) per grid-local heliostat
   const float4* subv;   // 3 float4 per sub-heliostat: A.xyz AB.x | AB.yz AC.xy | AC.z
-  const int* sub_free;  // per sub-heliostat: 1 when its facets' block walks can be skipped (qm::block_free)
+  // Per sub-heliostat, for its facets' block walks (qm::block_candidates):
+  // 1 = skipped (nothing can be hit), k + 1 = only the k <= kMaxCandidates
+  // heliostats in sub_cand[kMaxCandidates * sub ...] can be hit (a ray
+  // meeting none of their padded boxes skips the walk), 0 = walk.
+  const int* sub_free;
+  const int* sub_cand;
 };
 
 struct DevReceiver {
@@ -58,7 +67,12 @@ struct DevTask {
   const float4* samples;        // sun-shape pool already turned into world space by this task's sun
   const float4* perturbations;  // slope-error pool (local frame of the facet normal)
   int pool_size;                // P = groups x lights per group
-  int shadow_free;              // no ray of this heliostat can be shadowed: shadow walks skipped
+  // Shadow walks of this heliostat's rays (qm::cone_candidates around the
+  // sun-shape cone): 1 = skipped (nothing can shadow them), k + 1 = only the
+  // k listed heliostats can (a ray meeting none of their padded boxes skips
+  // its walk), 0 = walk.
+  int shadow_free;
+  int shadow_cand[kMaxCandidates];
 };
 
 struct SunFrame {
@@ -78,7 +92,7 @@ enum DiagSlot { kDiagClamped = 0, kDiagDdaCap = 1, kDiagSlots = 4 };
 // are one word per chunk iteration).  Larger chunks amortise the per-chunk
 // work (task lookup, facet window fill, power reduction) over more rays.
 #ifndef QM_CHUNK_ITERS
-#define QM_CHUNK_ITERS 8
+#define QM_CHUNK_ITERS 32
 #endif
 constexpr int kChunkIters = QM_CHUNK_ITERS;
 constexpr int kChunk = 32 * kChunkIters;

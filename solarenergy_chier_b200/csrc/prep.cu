@@ -62,6 +62,12 @@ __global__ void prep_kernel(const PrepItem* items, int n, DevTask* tasks) {
   *it.hsub = make_int4(it.sub_first, it.num_sub, rc.x, rc.y);
 }
 
+// DevGrid::sub_free code of a block_candidates result: 1 nothing to hit,
+// k + 1 for k listed candidates, 0 walk (too many, or not enumerable).
+__device__ __forceinline__ int candidate_code(int k) {
+  return k == 0 ? 1 : (k > 0 && k <= kMaxCandidates ? k + 1 : 0);
+}
+
 __global__ void shadow_kernel(const PrepItem* items, int n, DevTask* tasks, const DevGrid* grids) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -69,7 +75,9 @@ __global__ void shadow_kernel(const PrepItem* items, int n, DevTask* tasks, cons
   DevTask& T = tasks[it.task];
   const DevGrid& G = grids[T.grid];
   const ShadowGrid view{G.pos, G.interval, G.cells, G.bound, G.cell_range, G.entries};
-  T.shadow_free = it.shadow_tan >= 0.0f && shadow_free(view, T.own, it.shadow_axis, it.shadow_tan) ? 1 : 0;
+  T.shadow_free = candidate_code(it.shadow_tan >= 0.0f ? shadow_candidates(view, T.own, it.shadow_axis, it.shadow_tan,
+                                                                          T.shadow_cand, kMaxCandidates)
+                                                       : -1);
   Frame hf;
   hf.u = T.fu;
   hf.n = T.fn;
@@ -77,8 +85,11 @@ __global__ void shadow_kernel(const PrepItem* items, int n, DevTask* tasks, cons
   hf.identity = T.frame_identity != 0;
   for (int s = 0; s < it.num_sub; ++s) {
     const float3 n = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
-    it.sub_free[s] =
-        it.block_theta >= 0.0f && block_free(view, T.own, it.verts + 3 * s, it.sun_dir, n, it.block_theta) ? 1 : 0;
+    const int k = it.block_theta >= 0.0f ? block_candidates(view, T.own, it.verts + 3 * s, it.sun_dir, n,
+                                                           it.block_theta, it.sub_cand + kMaxCandidates * s,
+                                                           kMaxCandidates)
+                                         : -1;
+    it.sub_free[s] = candidate_code(k);
   }
 }
 
@@ -91,7 +102,10 @@ __global__ void walk_flags_kernel(WalkFlagParams p) {
   const DevTask& T = p.tasks[i];
   const DevGrid& G = p.grids[T.grid];
   const ShadowGrid view{G.pos, G.interval, G.cells, G.bound, G.cell_range, G.entries};
-  p.shadow_out[i] = p.sun_tan >= 0.0f && shadow_free(view, T.own, p.sun_axis, p.sun_tan) ? 1 : 0;
+  p.shadow_out[i] = candidate_code(p.sun_tan >= 0.0f ? shadow_candidates(view, T.own, p.sun_axis, p.sun_tan,
+                                                                         p.shadow_cand_out + kMaxCandidates * i,
+                                                                         kMaxCandidates)
+                                                      : -1);
   const int4 hs = G.hsub[T.own];
   Frame hf;
   hf.u = T.fu;
@@ -99,13 +113,17 @@ __global__ void walk_flags_kernel(WalkFlagParams p) {
   hf.v = T.fv;
   hf.identity = T.frame_identity != 0;
   int* sub_free = const_cast<int*>(G.sub_free);
+  int* sub_cand = const_cast<int*>(G.sub_cand);
   for (int s = 0; s < hs.y; ++s) {
     const float4* q = G.subv + 3 * (hs.x + s);
     const float3 A = make_float3(q[0].x, q[0].y, q[0].z);
     const float3 bac[3] = {make_float3(A.x + q[0].w, A.y + q[1].x, A.z + q[1].y), A,
                            make_float3(A.x + q[1].z, A.y + q[1].w, A.z + q[2].x)};
     const float3 n = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
-    sub_free[hs.x + s] = p.block_theta >= 0.0f && block_free(view, T.own, bac, p.sun_dir, n, p.block_theta) ? 1 : 0;
+    const int k = p.block_theta >= 0.0f ? block_candidates(view, T.own, bac, p.sun_dir, n, p.block_theta,
+                                                          sub_cand + kMaxCandidates * (hs.x + s), kMaxCandidates)
+                                        : -1;
+    sub_free[hs.x + s] = candidate_code(k);
   }
 }
 

@@ -30,6 +30,7 @@ struct PrepItem {
   // and where the heliostat's per-sub-heliostat flags go.
   float block_theta;
   int* sub_free;
+  int* sub_cand;  // kMaxCandidates per sub-heliostat
   float3* verts;    // out: 3 float3 (B, A, C) per sub-heliostat
   float4* subv;     // out: 3 float4 per sub-heliostat (A, B - A, C - A)
   float4* bound;    // out: 5 float4 traversal record
@@ -53,7 +54,8 @@ struct WalkFlagParams {
   float sun_tan;    // tan of the largest sun-shape angle (< 0: unbounded)
   float3 sun_dir;   // direction of travel
   float block_theta;
-  int* shadow_out;
+  int* shadow_out;       // per task: DevTask::shadow_free code
+  int* shadow_cand_out;  // per task: kMaxCandidates DevTask::shadow_cand entries
 };
 cudaError_t launch_walk_flags(const WalkFlagParams& p, cudaStream_t stream);
 

@@ -132,6 +132,20 @@ __device__ __forceinline__ bool box_window(const float4* b, const int4* hs, floa
   return true;
 }
 
+// The ray against a heliostat's padded box alone (the test box_window
+// opens with): false only if no point of the ray at t >= -1 is inside it.
+__device__ __forceinline__ bool box_meets(const float4* b, float3 o, float3 d) {
+  const float4 c = __ldg(b);
+  const float3 r = make_float3(o.x - c.x, o.y - c.y, o.z - c.z);
+  float tn = -3.0e38f, tf = 3.0e38f;
+#pragma unroll
+  for (int k = 1; k <= 3; ++k) {
+    const float4 ax = __ldg(b + k);
+    slab(r.x * ax.x + r.y * ax.y + r.z * ax.z, d.x * ax.x + d.y * ax.y + d.z * ax.z, ax.w, tn, tf);
+  }
+  return tn <= tf && tf >= -1.0f;
+}
+
 __device__ __forceinline__ bool sub_hit(const float4* sv, float3 o, float3 d) {
   float4 p0 = __ldg(sv), p1 = __ldg(sv + 1), p2 = __ldg(sv + 2);
   float t, u, v;
@@ -273,7 +287,8 @@ __device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, flo
 // (at most ceil(32/nl) + 1 <= 32 of them), so a warp keeps a window of 32
 // facets in shared memory -- origin, normal frame and the two pool offsets --
 // computed one facet per lane, and refills it only when an iteration needs a
-// facet past its end (once per chunk for nl >= 9).  Per-ray work then reads
+// facet past its end (once per 32 facets: once per chunk of 1,024 rays at
+// 32 lights per facet).  Per-ray work then reads
 // the window instead of re-deriving the facet, and holds no facet state in
 // registers across the grid walks.
 #ifndef QM_TRACE_THREADS
@@ -287,7 +302,7 @@ struct FacetWindow {
   // g in [0, P) plus a light index in [0, L) needs no wrap-around).
   const float4* samples[kThreads / 32];
   const float4* perturbations[kThreads / 32];
-  int shadow_free[kThreads / 32];  // the task's shadow walks can be skipped (qm::shadow_free)
+  int shadow_free[kThreads / 32];  // the task's shadow-walk code (DevTask::shadow_free)
   float4 o[kThreads];   // origin.xyz, pool offset g[f] (int bits)
   float4 u[kThreads];   // frame u.xyz, pool offset g[(f+1) % P] (int bits; bit 31: block walk skippable)
   float4 n[kThreads];   // frame n.xyz, frame identity flag
@@ -423,14 +438,19 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         const Frame fr = qs::make_frame(fnormal, false);
         win.o[wbase + lane] = make_float4(origin.x, origin.y, origin.z, __int_as_float(__ldg(T.offsets + fw)));
         // Pool offsets lie below 2^30; bit 31 carries the facet's
-        // sub-heliostat block-free flag (qm::block_free).
+        // sub-heliostat block-free flag, and the frame word below its
+        // candidate blockers (qm::block_candidates): n.w = sub-heliostat << 4
+        // | candidates << 1 | frame identity.
         const int per_row = T.row_col.y * T.sub_row_col.y;
         const int block = T.type == 1 ? (fw / per_row / T.sub_row_col.x) * T.row_col.y + (fw % per_row) / T.sub_row_col.y
                                       : 0;
-        const int free_bit = __ldg(G.sub_free + __ldg(&G.hsub[T.own].x) + block) ? (int)0x80000000 : 0;
+        const int sub = __ldg(&G.hsub[T.own].x) + block;
+        const int bcode = __ldg(G.sub_free + sub);
+        const int free_bit = bcode == 1 ? (int)0x80000000 : 0;
+        const int cands = bcode >= 2 ? bcode - 1 : 0;
         win.u[wbase + lane] = make_float4(fr.u.x, fr.u.y, fr.u.z,
                                           __int_as_float(__ldg(T.offsets + (fw + 1) % T.pool_size) | free_bit));
-        win.n[wbase + lane] = make_float4(fr.n.x, fr.n.y, fr.n.z, fr.identity ? 1.0f : 0.0f);
+        win.n[wbase + lane] = make_float4(fr.n.x, fr.n.y, fr.n.z, __int_as_float((sub << 4) | (cands << 1) | (fr.identity ? 1 : 0)));
         const WalkStart ws = walk_start(G, origin);
         win.v[wbase + lane] = make_float4(fr.v.x, fr.v.y, fr.v.z, __int_as_float(ws.cell.x));
         win.lo[wbase + lane] = make_float4(ws.lo.x, ws.lo.y, ws.lo.z, __int_as_float(ws.cell.y));
@@ -448,9 +468,17 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
       const float3 dir = xyz(__ldg(lds_ptr(win.samples[threadIdx.x >> 5]) + __float_as_int(win.o[slot].w) + lab));
       int32_t code;
       // Heliostats whose rays no other heliostat can shadow skip the shadow
-      // walk (qm::shadow_free, decided per sun when the task is built).
-      if (!lds_int(win.shadow_free[threadIdx.x >> 5]) &&
-          collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags)) {
+      // walk; where only a few listed heliostats can, a ray whose path meets
+      // none of their padded boxes skips it too (qm::cone_candidates,
+      // decided per sun when the task is built).
+      const int sc = lds_int(win.shadow_free[threadIdx.x >> 5]);
+      bool swalk = sc != 1;
+      if (sc >= 2) {
+        const float3 o = xyz(lds(win.o[slot]));
+        swalk = false;
+        for (int q = 0; q < sc - 1 && !swalk; ++q) swalk = box_meets(G.bound + 5 * __ldg(&T.shadow_cand[q]), o, dir);
+      }
+      if (swalk && collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags)) {
         code = kShadowed;
       } else {
         Frame nframe;
@@ -458,14 +486,28 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         const float4 wn = win.n[slot];
         nframe.n = xyz(wn);
         nframe.v = xyz(win.v[slot]);
-        nframe.identity = wn.w != 0.0f;
+        nframe.identity = (__float_as_int(wn.w) & 1) != 0;
         const int g1 = __float_as_int(lds(win.u[slot]).w);
         const int b = (g1 & 0x7fffffff) + lab;
         float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
         float3 rd = qs::normalize(qs::reflect(neg(dir), n));
         // Facets of sub-heliostats no other heliostat can block skip the
-        // block walk (qm::block_free, decided per sun with the pools).
-        if (g1 >= 0 && collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags)) {
+        // block walk (qm::block_candidates, decided per sun with the pools);
+        // where only a few listed heliostats can, a ray whose path meets
+        // none of their padded boxes skips it too (any blocker the walk
+        // could find is a listed heliostat whose box the ray enters).
+        bool walk = g1 >= 0;
+        if (walk) {
+          const int nw = __float_as_int(lds(win.n[slot]).w);
+          const int k = (nw >> 1) & 7;
+          if (k) {
+            const float3 o = xyz(lds(win.o[slot]));
+            const int* cand = G.sub_cand + kMaxCandidates * (nw >> 4);
+            walk = false;
+            for (int q = 0; q < k && !walk; ++q) walk = box_meets(G.bound + 5 * __ldg(cand + q), o, rd);
+          }
+        }
+        if (walk && collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags)) {
           code = kBlocked;
         } else {
           float tt, uu, vv;

@@ -177,13 +177,15 @@ class Scene:
         check(self._lib.qmcrt_set_light_range(self._h, begin, end))
 
     def shadow_free(self) -> np.ndarray:
-        """Per heliostat: 1 when its shadow walks are skipped for the current sun."""
+        """Per heliostat: 1 shadow walks skipped, k + 1 only k listed candidate
+        shadowing heliostats (rays missing their boxes skip the walk), 0 walk."""
         f = np.zeros(self.num_heliostats, np.int32)
         check(self._lib.qmcrt_debug_shadow_free(self._h, _ptr(f, ctypes.c_int)))
         return f
 
     def block_free(self, grid: int = 0) -> np.ndarray:
-        """Per sub-heliostat of a grid: 1 when its facets' block walks are skipped."""
+        """Per sub-heliostat of a grid: 1 block walks skipped, k + 1 only k listed
+        candidate blockers (rays missing their boxes skip the walk), 0 walk."""
         f = np.zeros(max(self.grid(grid)["num_sub"], 1), np.int32)
         check(self._lib.qmcrt_debug_block_free(self._h, grid, _ptr(f, ctypes.c_int)))
         return f

@@ -321,12 +321,15 @@ def test_shadow_skip_keeps_per_ray_outcomes(tmp_path, sun):
         got = c.scene.hit_records(h, 0, min(nf, 150), 0, L)
         want = o2.trace([h], c.dirs, c.pert, c.offsets, record=(h, 0, min(nf, 150)), images=False)["records"]
         assert np.array_equal(got, want), f"heliostat {h} (shadow-free {flags[h]}): {np.mean(got != want):.2e} differ"
-        if flags[h]:
+        if flags[h] == 1:
             assert not np.any(want == -1), f"heliostat {h} flagged shadow-free but the oracle shadows rays"
         shadowed += int(np.sum(want == -1))
     bfree = c.scene.block_free(0)
-    print("sun", sun, "shadow-free heliostats", int(flags.sum()), "of", len(flags), "shadowed rays", shadowed,
-          "block-free sub-heliostats", int(bfree.sum()), "of", len(bfree))
+    print("sun", sun, "shadow-free heliostats", int((flags == 1).sum()), "with candidate lists",
+          int((flags >= 2).sum()), "of", len(flags), "shadowed rays", shadowed,
+          "block-free sub-heliostats", int((bfree == 1).sum()), "with candidate lists", int((bfree >= 2).sum()),
+          "of", len(bfree))
+    assert set(np.unique(bfree)) <= set(range(0, 8))
 
 
 def test_sharded_trace_one_rank_equals_plain(small):
