@@ -32,8 +32,9 @@ forward + adjoint over 32 suns of a 10,000-heliostat field.
 `aim_optimisation` (--adam-steps K, default 0 = skipped) runs K Adam steps
 of aim-point optimisation on the field's 624 x 2 aim offsets, each step
 checked by the plain tracer on the same parameters.
-`reference_cuda` (--reference-cuda N) times the reference's own CUDA build
-on N heliostats spread over the field, and this tracer on the same ones.
+The reference's own CUDA build is timed beside this tracer by
+tests/test_gpu_reference.py (it runs from oracle/, which only the tests and
+the CPU baseline below execute).
 
 --impl reference times the reference's own per-ray routine (its host code
 compiled from the reference tree, OpenMP over all host cores) on a bounded
@@ -83,8 +84,6 @@ def parse_args():
     p.add_argument("--exact", action="store_true", help="time the kernel build without FMA contraction")
     p.add_argument("--mode", type=int, default=None, help="kernel build: 0 production, 1 exact, 2 production/48 regs")
     p.add_argument("--heliostats", type=int, default=0, help="trace only the first N heliostats (profiling)")
-    p.add_argument("--reference-cuda", type=int, default=0, metavar="N",
-                   help="also time the reference's own CUDA tracer on N heliostats spread over the field")
     return p.parse_args()
 
 
@@ -148,33 +147,12 @@ def fp32_peak_tflops(torch) -> float:
     return microbench.fp32_fma_tflops()
 
 
-def census(files, lights: int = 8, stride: int = 4001):
-    """Algorithmic work per ray on a fixed subsample, counted by the CPU oracle:
-    parallelogram tests reaching each stage, grid cells visited, receiver hits."""
-    from oracle import oracle as orc
-
-    import numpy as np
-
-    o = orc.OracleScene.from_files(files.scene, files.config)
-    P = o.pool_size
-    rng = np.random.default_rng(5)
-    th = 0.00465 * np.sqrt(rng.random(P))
-    ph = 2 * np.pi * rng.random(P)
-    dirs = np.stack([np.sin(th) * np.cos(ph), np.cos(th), np.sin(th) * np.sin(ph)], 1).astype(np.float32)
-    pert = np.tile(np.array([0, 1, 0], np.float32), (P, 1))
-    offs = {h: rng.integers(0, P, o.heliostat(h)["num_facets"] + 1).astype(np.int32) for h in range(o.num_heliostats)}
-    res = o.trace(list(range(o.num_heliostats)), dirs, pert, offs, 0, lights, facet_stride=stride, images=False)
-    c = res["counters"]
-    n = max(c["rays"], 1)
-    per = {k: c[k] / n for k in ("tests_det", "tests_u", "tests_v", "tests_t", "cells", "hit", "shadowed", "blocked",
-                                 "missed")}
-    # flops per ray credited per executed stage (23 det, 6 u, 15 v, 6 t), 20 per cell step,
-    # 70 for sampling/perturbation/reflection, 55 for the cylinder test when reached
-    reach_receiver = (c["hit"] + c["missed"]) / n
-    per["flops"] = (23 * per["tests_det"] + 6 * per["tests_u"] + 15 * per["tests_v"] + 6 * per["tests_t"]
-                    + 20 * per["cells"] + 70 + 55 * reach_receiver)
-    per["rays_sampled"] = n
-    return per
+def census():
+    """Algorithmic work per ray of the reference algorithm on this field (parallelogram
+    tests reaching each stage, grid cells visited, receiver hits, FP32 flops),
+    counted once by the CPU oracle and frozen in tests/golden/work_per_ray_624field.json
+    (tests/golden/make_work_census.py)."""
+    return json.loads((ROOT / "tests" / "golden" / "work_per_ray_624field.json").read_text())
 
 
 def batched_vs_plain(torch, scene, lights: int, stream, num_fields: int = 16, seed: int = 0):
@@ -385,14 +363,26 @@ def large_adjoint(torch, lights: int, num_suns: int, stream, seed: int = 0):
     free_b, total_b = torch.cuda.mem_get_info()
     used = int(total_b - free_b)
     recomputed, ckpt = d.hit_records()
+    d.close()
+    # the plain tracer on the same instances and rays (nearest-pixel flux)
+    batch = q.Batch([scene], [(0, sun) for sun in suns])
+    batch.set_light_range(0, lights)
+    batch.trace(stream)
+    torch.cuda.synchronize()
+    e[0].record(stream)
+    batch.trace(stream)
+    e[1].record(stream)
+    torch.cuda.synchronize()
+    plain = e[0].elapsed_time(e[1])
+    batch.close()
     rays = facets * lights * len(suns)
     out = {"heliostats": H, "facets_per_heliostat": facets // H, "suns": len(suns), "lights_per_sun": lights,
            "rays_per_sun": facets * lights, "rays": rays, "forward_ms": fwd, "adjoint_ms": bwd,
            "adjoint_over_forward": bwd / fwd, "forward_mrays_s": rays / (fwd / 1e3) / 1e6,
            "hit_records": "recomputed" if recomputed else "checkpointed", "checkpoint_bytes": ckpt,
            "device_memory_used_bytes": used,
+           "plain_batch_trace_ms": plain, "forward_over_plain": fwd / plain,
            "loss": loss, "grad_norm": float(np.linalg.norm(grad))}
-    d.close()
     scene.close()
     return out
 
@@ -405,43 +395,6 @@ def cpu_baseline(files, seconds: float):
     if out.returncode != 0:
         raise RuntimeError(out.stderr.strip().splitlines()[-1] if out.stderr.strip() else "cpu baseline failed")
     return json.loads(out.stdout.strip().splitlines()[-1])
-
-
-def reference_cuda(files, scene, count: int):
-    """The reference's CUDA tracer on `count` heliostats spread over the field
-    (oracle/ref_gpu_bench.py, own process), and this tracer on the same ones."""
-    import torch
-
-    nh = scene.num_heliostats
-    ids = sorted({int(round(i * (nh - 1) / max(count - 1, 1))) for i in range(count)})
-    try:
-        out = subprocess.run([sys.executable, "-m", "oracle.ref_gpu_bench", str(files.scene), str(files.config),
-                              *map(str, ids)], capture_output=True, text=True, cwd=str(ROOT), timeout=1200)
-        lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
-        if not lines:
-            tail = (out.stderr or "").strip().splitlines()[-3:]
-            return {"unavailable": f"reference CUDA run exited {out.returncode}: {' | '.join(tail)}"}
-        ref = json.loads(lines[-1])
-    except Exception as exc:
-        return {"unavailable": f"reference CUDA run failed: {exc}"}
-    if "unavailable" in ref:
-        return ref
-    # this tracer on the same heliostats, all 2048 lights, one launch
-    L = scene.lights_per_group
-    scene.set_light_range(0, L)
-    scene.trace(ids)
-    torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    scene.trace(ids)
-    b.record()
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b)
-    ref["this_tracer_ms"] = ms
-    ref["this_tracer_mrays_s"] = ref["rays"] / (ms / 1e3) / 1e6
-    ref["speedup_vs_reference_kernel"] = ref["this_tracer_mrays_s"] / ref["kernel_mrays_s"]
-    ref["speedup_vs_reference_pipeline"] = ref["this_tracer_mrays_s"] / ref["pipeline_mrays_s"]
-    return ref
 
 
 def run_reference(args):
@@ -565,7 +518,7 @@ def main():
     d2h = img.nbytes + per.nbytes
 
     if rank == 0:
-        per_ray = census(files)
+        per_ray = census()
         fp32_peak = fp32_peak_tflops(torch)
         achieved_tflops = value * 1e6 * per_ray["flops"] / 1e12
         from solarenergy_chier_b200 import microbench
@@ -610,8 +563,6 @@ def main():
             line["large_adjoint"] = large_adjoint(torch, args.large_adjoint_lights, 32, stream)
         if args.adam_steps > 0:
             line["aim_optimisation"] = aim_optimisation(torch, scene, args.adam_steps, args.adam_lights, stream)
-        if args.reference_cuda > 0:
-            line["reference_cuda"] = reference_cuda(files, scene, args.reference_cuda)
         if not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(files, args.cpu_seconds)

@@ -37,7 +37,7 @@ struct qmcrt_diff {
   int H = 0;
   int suns = 1;
   int hit_mode = 0;                       // 0 automatic, 1 checkpoint, 2 recompute
-  long long segment_chunks = 1LL << 20;   // warp chunks per recompute segment (256 rays each)
+  long long segment_chunks = (1LL << 28) / qm::kChunk;  // warp chunks per recompute segment (2^28 rays)
   bool recompute = false;                 // the last forward's choice
   size_t n_slots = 0;                     // power slots of the batch (suns x heliostats)
   int radius = 0;
@@ -245,7 +245,7 @@ int qmcrt_fwd(qmcrt_diff* d, double* loss, void* stream) {
                                     d->d_dtasks.as<qm::DiffTask>(), st),
                "diff preparation");
     if (b->total_chunks < 0) batch_build_prefix(b);
-    const size_t bits_bytes = (size_t)std::max<long long>(b->total_chunks, 1) * 8 * sizeof(uint32_t);
+    const size_t bits_bytes = (size_t)std::max<long long>(b->total_chunks, 1) * qm::kChunkIters * sizeof(uint32_t);
     if (d->hit_mode == 0) {
       size_t free_b = 0, total_b = 0;
       cuda_check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
@@ -255,7 +255,7 @@ int qmcrt_fwd(qmcrt_diff* d, double* loss, void* stream) {
     }
     if (d->recompute) {
       b->hit_bits = nullptr;  // the adjoint recomputes them
-      if (d->d_bits.bytes > (size_t)d->segment_chunks * 8 * sizeof(uint32_t)) d->d_bits.release();
+      if (d->d_bits.bytes > (size_t)d->segment_chunks * qm::kChunkIters * sizeof(uint32_t)) d->d_bits.release();
     } else {
       d->d_bits.alloc(bits_bytes);
       b->hit_bits = d->d_bits.as<uint32_t>();
@@ -319,7 +319,8 @@ int qmcrt_bwd(qmcrt_diff* d, double* grad, void* stream) {
       // segment's chunks (the forward's kernel, mode and rays), then the
       // adjoint over the same chunks.
       const long long seg = std::max<long long>(1, d->segment_chunks);
-      d->d_bits.alloc((size_t)std::min(seg, std::max<long long>(b->total_chunks, 1)) * 8 * sizeof(uint32_t));
+      d->d_bits.alloc((size_t)std::min(seg, std::max<long long>(b->total_chunks, 1)) * qm::kChunkIters *
+                     sizeof(uint32_t));
       b->hit_bits = d->d_bits.as<uint32_t>();
       for (long long c0 = 0; c0 < b->total_chunks; c0 += seg) {
         const long long c1 = std::min(b->total_chunks, c0 + seg);

@@ -181,6 +181,40 @@ __device__ __forceinline__ bool cell_hit(const DevGrid& g, int cell, int own, fl
   return false;
 }
 
+// Whether the ray hits any sub-heliostat of heliostat h (the test cell_hit
+// makes for each heliostat listed in a cell).
+__device__ __forceinline__ bool heliostat_hit(const DevGrid& g, int h, float3 o, float3 d) {
+  const int4 hs = __ldg(g.hsub + h);  // first, count, rows, columns
+  if (hs.y == 1) return sub_hit(g.subv + 3 * hs.x, o, d);
+  int r0, r1, c0, c1, cols;
+  if (!box_window(g.bound + 5 * h, g.hsub + h, o, d, r0, r1, c0, c1, cols)) return false;
+  for (int rr = r0; rr <= r1; ++rr)
+    for (int cc = c0; cc <= c1; ++cc)
+      if (sub_hit(g.subv + 3 * (hs.x + rr * cols + cc), o, d)) return true;
+  return false;
+}
+
+// Any-hit of a ray whose possible blockers are the k listed heliostats
+// cand[0..k) (the walk-free tests' candidate lists, 1 <= k): whether the
+// reference's walk can find a hit at all.  The production builds
+// (QM_TRACE_CANDIDATE_HITS) answer it directly by testing the listed
+// heliostats -- the walk visits every cell the ray crosses, so it tests every
+// heliostat the ray can hit and finds the same answer, except where a 1e-5
+// tie makes it step two axes at once past a cell corner the hit lies in.
+// The exact build returns -1 (walk) unless the ray misses every listed
+// heliostat's padded box, then 0 (no hit, the walk skipped).
+__device__ __forceinline__ int candidate_hit(const DevGrid& g, const int* cand, int k, float3 o, float3 d) {
+#if defined(QM_TRACE_CANDIDATE_HITS)
+  for (int q = 0; q < k; ++q)
+    if (heliostat_hit(g, __ldg(cand + q), o, d)) return 1;
+  return 0;
+#else
+  for (int q = 0; q < k; ++q)
+    if (box_meets(g.bound + 5 * __ldg(cand + q), o, d)) return -1;
+  return 0;
+#endif
+}
+
 // rectGridDDA::collision (rectGridDDA.cu:31-119).  The reference loops until
 // the walk leaves the grid; a walk that stops advancing (an exact tie the
 // reference never leaves) or exceeds cells.x+cells.y+cells.z+2 steps ends
@@ -468,17 +502,13 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
       const float3 dir = xyz(__ldg(lds_ptr(win.samples[threadIdx.x >> 5]) + __float_as_int(win.o[slot].w) + lab));
       int32_t code;
       // Heliostats whose rays no other heliostat can shadow skip the shadow
-      // walk; where only a few listed heliostats can, a ray whose path meets
-      // none of their padded boxes skips it too (qm::cone_candidates,
-      // decided per sun when the task is built).
+      // walk; where only a few listed heliostats can (qm::cone_candidates,
+      // decided per sun when the task is built), candidate_hit decides.
       const int sc = lds_int(win.shadow_free[threadIdx.x >> 5]);
-      bool swalk = sc != 1;
-      if (sc >= 2) {
-        const float3 o = xyz(lds(win.o[slot]));
-        swalk = false;
-        for (int q = 0; q < sc - 1 && !swalk; ++q) swalk = box_meets(G.bound + 5 * __ldg(&T.shadow_cand[q]), o, dir);
-      }
-      if (swalk && collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags)) {
+      int shadowed = sc == 1 ? 0 : -1;  // -1: walk
+      if (sc >= 2) shadowed = candidate_hit(G, T.shadow_cand, sc - 1, xyz(lds(win.o[slot])), dir);
+      if (shadowed < 0) shadowed = collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags);
+      if (shadowed) {
         code = kShadowed;
       } else {
         Frame nframe;
@@ -492,22 +522,17 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
         float3 rd = qs::normalize(qs::reflect(neg(dir), n));
         // Facets of sub-heliostats no other heliostat can block skip the
-        // block walk (qm::block_candidates, decided per sun with the pools);
-        // where only a few listed heliostats can, a ray whose path meets
-        // none of their padded boxes skips it too (any blocker the walk
-        // could find is a listed heliostat whose box the ray enters).
-        bool walk = g1 >= 0;
-        if (walk) {
+        // block walk; where only a few listed heliostats can
+        // (qm::block_candidates, decided per sun with the pools),
+        // candidate_hit decides.
+        int blocked = 0;
+        if (g1 >= 0) {
           const int nw = __float_as_int(lds(win.n[slot]).w);
           const int k = (nw >> 1) & 7;
-          if (k) {
-            const float3 o = xyz(lds(win.o[slot]));
-            const int* cand = G.sub_cand + kMaxCandidates * (nw >> 4);
-            walk = false;
-            for (int q = 0; q < k && !walk; ++q) walk = box_meets(G.bound + 5 * __ldg(cand + q), o, rd);
-          }
+          blocked = k ? candidate_hit(G, G.sub_cand + kMaxCandidates * (nw >> 4), k, xyz(lds(win.o[slot])), rd) : -1;
+          if (blocked < 0) blocked = collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags);
         }
-        if (walk && collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags)) {
+        if (blocked) {
           code = kBlocked;
         } else {
           float tt, uu, vv;

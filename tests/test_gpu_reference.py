@@ -91,3 +91,39 @@ def test_flux_against_the_reference_cuda_tracer(which, tmp_path, cuda_device):
         assert abs(total - host.sum()) <= 1e-5 * host.sum()
         assert ours_vs_gpu <= max(1e-3, 1.05 * gpu_vs_host)
         assert ours_vs_fp64 <= 1.05 * gpu_vs_fp64 + 1e-4
+
+
+@pytest.mark.skipif(not LIB.exists(), reason="the reference's CUDA build (oracle/_ref/libref_gpu.so) is absent")
+def test_throughput_against_the_reference_cuda_tracer(tmp_path, cuda_device):
+    """Rays per second of the reference's CUDA tracer and of this tracer on the
+    same 16 heliostats spread over the 624-heliostat field, all 2048 light
+    indexes (oracle/ref_gpu_bench.py, own process: QuasiMonteCarloRayTracer::
+    rayTracing per heliostat end to end, and its map_raytracing launch alone).
+    Bar (the north star's): at least 3x the reference kernel's rays/s."""
+    import json
+
+    import torch
+
+    files = synth.large_field(tmp_path, seed=0)
+    s = q.Scene(files.scene, files.config, device=0, seed=0)
+    nh, count = s.num_heliostats, 16
+    ids = sorted({int(round(i * (nh - 1) / (count - 1))) for i in range(count)})
+    r = subprocess.run([sys.executable, "-m", "oracle.ref_gpu_bench", str(files.scene), str(files.config),
+                        *map(str, ids)], cwd=str(ROOT), capture_output=True, text=True, timeout=1200)
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    assert lines, r.stdout[-2000:] + r.stderr[-2000:]
+    ref = json.loads(lines[-1])
+    assert "unavailable" not in ref, ref
+    s.set_light_range(0, s.lights_per_group)
+    s.trace(ids)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    s.trace(ids)
+    b.record()
+    torch.cuda.synchronize()
+    ours = ref["rays"] / (a.elapsed_time(b) / 1e3) / 1e6
+    print(f"reference CUDA: kernel {ref['kernel_mrays_s']:.0f} Mrays/s, rayTracing loop {ref['pipeline_mrays_s']:.0f} "
+          f"Mrays/s; this tracer {ours:.0f} Mrays/s ({ours / ref['kernel_mrays_s']:.1f}x the kernel, "
+          f"{ours / ref['pipeline_mrays_s']:.1f}x the loop) on {ref['rays']:.3e} rays")
+    assert ours >= 3.0 * ref["kernel_mrays_s"]
