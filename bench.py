@@ -83,7 +83,9 @@ def parse_args():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--exact", action="store_true", help="time the kernel build without FMA contraction")
     p.add_argument("--mode", type=int, default=None, help="kernel build: 0 production, 1 exact, 2 production/48 regs")
-    p.add_argument("--heliostats", type=int, default=0, help="trace only the first N heliostats (profiling)")
+    p.add_argument("--heliostats", type=int, default=0, help="trace only N heliostats (profiling)")
+    p.add_argument("--heliostat-stride", type=int, default=1,
+                   help="with --heliostats: take every S-th heliostat, spreading the slice over the field")
     return p.parse_args()
 
 
@@ -448,7 +450,7 @@ def main():
     L = scene.lights_per_group
     P = scene.pool_size
     nh = scene.num_heliostats
-    ids = list(range(nh if args.heliostats <= 0 else min(nh, args.heliostats)))
+    ids = list(range(nh)) if args.heliostats <= 0 else list(range(0, nh, max(1, args.heliostat_stride)))[:args.heliostats]
     total_facets = sum(scene.heliostat(h)["num_facets"] for h in ids)
     passes = max(1, min(args.passes, L))
     stream = torch.cuda.Stream()

@@ -79,8 +79,10 @@ void batch_prepare(qmcrt_batch* b, cudaStream_t st) {
              "prep upload");
   cuda_check(qm::launch_prep(b->d_items.as<qm::PrepItem>(), (int)b->items.size(), b->d_tasks.as<qm::DevTask>(), st),
              "prep kernel");
-  cuda_check(qm::launch_shadow_flags(b->d_items.as<qm::PrepItem>(), (int)b->items.size(), b->d_tasks.as<qm::DevTask>(),
-                                     b->d_grids.as<qm::DevGrid>(), st),
+  int max_sub = 0;
+  for (const auto& it : b->items) max_sub = std::max(max_sub, it.num_sub);
+  cuda_check(qm::launch_shadow_flags(b->d_items.as<qm::PrepItem>(), (int)b->items.size(), max_sub,
+                                     b->d_tasks.as<qm::DevTask>(), b->d_grids.as<qm::DevGrid>(), st),
              "shadow flags");
   std::vector<qm::PoolRotation> rot(b->inst.size());
   int max_out = 0;

@@ -295,6 +295,8 @@ void update_shadow_flags(qmcrt_scene* s, bool pools_changed) {
   s->d_flag_out.alloc(std::max<size_t>(s->templates.size(), 1) * (1 + qm::kMaxCandidates) * sizeof(int));
   p.tasks = s->d_flag_tasks.as<DevTask>();
   p.n = (int)s->templates.size();
+  p.max_sub = 0;
+  for (const auto& h : s->model.heliostats) p.max_sub = std::max(p.max_sub, h.num_sub);
   p.grids = s->d_grids.as<DevGrid>();
   p.sun_axis = axis;
   p.sun_tan = tan_world;

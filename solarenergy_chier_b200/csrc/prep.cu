@@ -68,45 +68,60 @@ __device__ __forceinline__ int candidate_code(int k) {
   return k == 0 ? 1 : (k > 0 && k <= kMaxCandidates ? k + 1 : 0);
 }
 
-__global__ void shadow_kernel(const PrepItem* items, int n, DevTask* tasks, const DevGrid* grids) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// Walk codes of the prepared tasks: thread j handles task j / (1 + max_sub),
+// slot j % (1 + max_sub): slot 0 its shadow walks, slot 1 + s the block
+// walks of its sub-heliostat s (each a capsule enumeration of its own).
+__global__ void shadow_kernel(const PrepItem* items, int n, int max_sub, DevTask* tasks, const DevGrid* grids) {
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(j / (1 + max_sub)), slot = (int)(j % (1 + max_sub));
   if (i >= n) return;
-  const PrepItem it = items[i];
+  const PrepItem& it = items[i];
   DevTask& T = tasks[it.task];
   const DevGrid& G = grids[T.grid];
   const ShadowGrid view{G.pos, G.interval, G.cells, G.bound, G.cell_range, G.entries};
-  T.shadow_free = candidate_code(it.shadow_tan >= 0.0f ? shadow_candidates(view, T.own, it.shadow_axis, it.shadow_tan,
-                                                                          T.shadow_cand, kMaxCandidates)
-                                                       : -1);
+  if (slot == 0) {
+    T.shadow_free = candidate_code(it.shadow_tan >= 0.0f ? shadow_candidates(view, T.own, it.shadow_axis,
+                                                                            it.shadow_tan, T.shadow_cand,
+                                                                            kMaxCandidates)
+                                                         : -1);
+    return;
+  }
+  const int s = slot - 1;
+  if (s >= it.num_sub) return;
   Frame hf;
   hf.u = T.fu;
   hf.n = T.fn;
   hf.v = T.fv;
   hf.identity = T.frame_identity != 0;
-  for (int s = 0; s < it.num_sub; ++s) {
-    const float3 n = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
-    const int k = it.block_theta >= 0.0f ? block_candidates(view, T.own, it.verts + 3 * s, it.sun_dir, n,
-                                                           it.block_theta, it.sub_cand + kMaxCandidates * s,
-                                                           kMaxCandidates)
-                                         : -1;
-    it.sub_free[s] = candidate_code(k);
-  }
+  const float3 nrm = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
+  const int k = it.block_theta >= 0.0f ? block_candidates(view, T.own, it.verts + 3 * s, it.sun_dir, nrm,
+                                                         it.block_theta, it.sub_cand + kMaxCandidates * s,
+                                                         kMaxCandidates)
+                                       : -1;
+  it.sub_free[s] = candidate_code(k);
 }
 
-// Walk-free flags of a plain scene's heliostats (its task templates); the
-// sub-heliostat parallelograms are read back from the traversal form
-// (A, B - A, C - A) -- the tests are conservative far above that rounding.
+// Walk codes of a plain scene's heliostats (its task templates), with the
+// same thread layout as shadow_kernel; the sub-heliostat parallelograms are
+// read back from the traversal form (A, B - A, C - A) -- the tests are
+// conservative far above that rounding.
 __global__ void walk_flags_kernel(WalkFlagParams p) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long j = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(j / (1 + p.max_sub)), slot = (int)(j % (1 + p.max_sub));
   if (i >= p.n) return;
   const DevTask& T = p.tasks[i];
   const DevGrid& G = p.grids[T.grid];
   const ShadowGrid view{G.pos, G.interval, G.cells, G.bound, G.cell_range, G.entries};
-  p.shadow_out[i] = candidate_code(p.sun_tan >= 0.0f ? shadow_candidates(view, T.own, p.sun_axis, p.sun_tan,
-                                                                         p.shadow_cand_out + kMaxCandidates * i,
-                                                                         kMaxCandidates)
-                                                      : -1);
+  if (slot == 0) {
+    p.shadow_out[i] = candidate_code(p.sun_tan >= 0.0f ? shadow_candidates(view, T.own, p.sun_axis, p.sun_tan,
+                                                                           p.shadow_cand_out + kMaxCandidates * i,
+                                                                           kMaxCandidates)
+                                                        : -1);
+    return;
+  }
+  const int s = slot - 1;
   const int4 hs = G.hsub[T.own];
+  if (s >= hs.y) return;
   Frame hf;
   hf.u = T.fu;
   hf.n = T.fn;
@@ -114,17 +129,15 @@ __global__ void walk_flags_kernel(WalkFlagParams p) {
   hf.identity = T.frame_identity != 0;
   int* sub_free = const_cast<int*>(G.sub_free);
   int* sub_cand = const_cast<int*>(G.sub_cand);
-  for (int s = 0; s < hs.y; ++s) {
-    const float4* q = G.subv + 3 * (hs.x + s);
-    const float3 A = make_float3(q[0].x, q[0].y, q[0].z);
-    const float3 bac[3] = {make_float3(A.x + q[0].w, A.y + q[1].x, A.z + q[1].y), A,
-                           make_float3(A.x + q[1].z, A.y + q[1].w, A.z + q[2].x)};
-    const float3 n = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
-    const int k = p.block_theta >= 0.0f ? block_candidates(view, T.own, bac, p.sun_dir, n, p.block_theta,
-                                                          sub_cand + kMaxCandidates * (hs.x + s), kMaxCandidates)
-                                        : -1;
-    sub_free[hs.x + s] = candidate_code(k);
-  }
+  const float4* q = G.subv + 3 * (hs.x + s);
+  const float3 A = make_float3(q[0].x, q[0].y, q[0].z);
+  const float3 bac[3] = {make_float3(A.x + q[0].w, A.y + q[1].x, A.z + q[1].y), A,
+                         make_float3(A.x + q[1].z, A.y + q[1].w, A.z + q[2].x)};
+  const float3 nrm = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
+  const int k = p.block_theta >= 0.0f ? block_candidates(view, T.own, bac, p.sun_dir, nrm, p.block_theta,
+                                                        sub_cand + kMaxCandidates * (hs.x + s), kMaxCandidates)
+                                      : -1;
+  sub_free[hs.x + s] = candidate_code(k);
 }
 
 // Pool of instance blockIdx.y turned by that instance's sun frame.
@@ -153,16 +166,20 @@ cudaError_t launch_prep(const PrepItem* items, int n, DevTask* tasks, cudaStream
   return cudaGetLastError();
 }
 
-cudaError_t launch_shadow_flags(const PrepItem* items, int n, DevTask* tasks, const DevGrid* grids,
+cudaError_t launch_shadow_flags(const PrepItem* items, int n, int max_sub, DevTask* tasks, const DevGrid* grids,
                                 cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
-  shadow_kernel<<<(n + 127) / 128, 128, 0, stream>>>(items, n, tasks, grids);
+  if (max_sub < 0) return cudaErrorInvalidValue;
+  const long long threads = (long long)n * (1 + max_sub);
+  shadow_kernel<<<(unsigned)((threads + 63) / 64), 64, 0, stream>>>(items, n, max_sub, tasks, grids);
   return cudaGetLastError();
 }
 
 cudaError_t launch_walk_flags(const WalkFlagParams& p, cudaStream_t stream) {
   if (p.n <= 0) return cudaSuccess;
-  walk_flags_kernel<<<(p.n + 63) / 64, 64, 0, stream>>>(p);
+  if (p.max_sub < 0) return cudaErrorInvalidValue;
+  const long long threads = (long long)p.n * (1 + p.max_sub);
+  walk_flags_kernel<<<(unsigned)((threads + 63) / 64), 64, 0, stream>>>(p);
   return cudaGetLastError();
 }
 

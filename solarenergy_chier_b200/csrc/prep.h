@@ -56,13 +56,16 @@ struct WalkFlagParams {
   float block_theta;
   int* shadow_out;       // per task: DevTask::shadow_free code
   int* shadow_cand_out;  // per task: kMaxCandidates DevTask::shadow_cand entries
+  int max_sub;           // most sub-heliostats of any task
 };
 cudaError_t launch_walk_flags(const WalkFlagParams& p, cudaStream_t stream);
 
 cudaError_t launch_prep(const PrepItem* items, int n, DevTask* tasks, cudaStream_t stream);
 // Shadow-free flags of the prepared tasks; grids: the tasks' grids with their
 // prepared traversal records.  Run after launch_prep.
-cudaError_t launch_shadow_flags(const PrepItem* items, int n, DevTask* tasks, const DevGrid* grids,
+// max_sub: the most sub-heliostats of any item (one thread per heliostat and
+// per sub-heliostat).
+cudaError_t launch_shadow_flags(const PrepItem* items, int n, int max_sub, DevTask* tasks, const DevGrid* grids,
                                 cudaStream_t stream);
 // max_out: the largest n_out of the jobs.
 cudaError_t launch_rotate_pools(const PoolRotation* jobs, int n_jobs, int max_out, cudaStream_t stream);

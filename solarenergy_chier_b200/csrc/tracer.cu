@@ -221,8 +221,7 @@ __device__ __forceinline__ int candidate_hit(const DevGrid& g, const int* cand, 
 // here with "no hit" and a diagnostic count instead.
 // Start of a walk from origin o: its cell, and per axis the distances to the
 // cell's lower and upper boundary (rectGridDDA.cu:36-52; calTMax with
-// dir < 0 and dir >= 0).  It depends on the origin only, so both walks of a
-// ray, and every ray of a facet, share it.
+// dir < 0 and dir >= 0).  It depends on the origin only.
 struct WalkStart {
   int3 cell;
   float3 lo, hi;
@@ -339,10 +338,8 @@ struct FacetWindow {
   int shadow_free[kThreads / 32];  // the task's shadow-walk code (DevTask::shadow_free)
   float4 o[kThreads];   // origin.xyz, pool offset g[f] (int bits)
   float4 u[kThreads];   // frame u.xyz, pool offset g[(f+1) % P] (int bits; bit 31: block walk skippable)
-  float4 n[kThreads];   // frame n.xyz, frame identity flag
-  float4 v[kThreads];   // frame v.xyz, walk start cell x (int bits)
-  float4 lo[kThreads];  // walk start distances to the lower cell boundaries, cell y
-  float4 hi[kThreads];  // distances to the upper cell boundaries, cell z
+  float4 n[kThreads];   // frame n.xyz, sub-heliostat << 4 | candidate blockers << 1 | frame identity (int bits)
+  float4 v[kThreads];   // frame v.xyz
 };
 
 // Shared-memory read the compiler may not merge with an earlier read of the
@@ -369,13 +366,10 @@ __device__ __forceinline__ const float4* lds_ptr(const float4* const& x) {
   return reinterpret_cast<const float4*>(r);
 }
 
-__device__ __forceinline__ WalkStart window_start(const FacetWindow& win, int slot) {
-  const float4 lo = lds(win.lo[slot]), hi = lds(win.hi[slot]);
-  WalkStart ws;
-  ws.cell = make_int3(__float_as_int(lds(win.v[slot]).w), __float_as_int(lo.w), __float_as_int(hi.w));
-  ws.lo = xyz(lo);
-  ws.hi = xyz(hi);
-  return ws;
+// DDA start of a facet's walks, computed from its origin when a ray walks
+// (most rays decide shadowing and blocking without a walk).
+__device__ __forceinline__ WalkStart window_start(const DevGrid& g, const FacetWindow& win, int slot) {
+  return walk_start(g, xyz(lds(win.o[slot])));
 }
 
 // Output of a launch: flux into the receiver images (nearest pixel, the
@@ -485,10 +479,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         win.u[wbase + lane] = make_float4(fr.u.x, fr.u.y, fr.u.z,
                                           __int_as_float(__ldg(T.offsets + (fw + 1) % T.pool_size) | free_bit));
         win.n[wbase + lane] = make_float4(fr.n.x, fr.n.y, fr.n.z, __int_as_float((sub << 4) | (cands << 1) | (fr.identity ? 1 : 0)));
-        const WalkStart ws = walk_start(G, origin);
-        win.v[wbase + lane] = make_float4(fr.v.x, fr.v.y, fr.v.z, __int_as_float(ws.cell.x));
-        win.lo[wbase + lane] = make_float4(ws.lo.x, ws.lo.y, ws.lo.z, __int_as_float(ws.cell.y));
-        win.hi[wbase + lane] = make_float4(ws.hi.x, ws.hi.y, ws.hi.z, __int_as_float(ws.cell.z));
+        win.v[wbase + lane] = make_float4(fr.v.x, fr.v.y, fr.v.z, 0.0f);
       }
       __syncwarp();
     }
@@ -507,7 +498,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
       const int sc = lds_int(win.shadow_free[threadIdx.x >> 5]);
       int shadowed = sc == 1 ? 0 : -1;  // -1: walk
       if (sc >= 2) shadowed = candidate_hit(G, T.shadow_cand, sc - 1, xyz(lds(win.o[slot])), dir);
-      if (shadowed < 0) shadowed = collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(win, slot), flags);
+      if (shadowed < 0) shadowed = collide(G, T.own, xyz(lds(win.o[slot])), dir, window_start(G, win, slot), flags);
       if (shadowed) {
         code = kShadowed;
       } else {
@@ -530,7 +521,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
           const int nw = __float_as_int(lds(win.n[slot]).w);
           const int k = (nw >> 1) & 7;
           blocked = k ? candidate_hit(G, G.sub_cand + kMaxCandidates * (nw >> 4), k, xyz(lds(win.o[slot])), rd) : -1;
-          if (blocked < 0) blocked = collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(win, slot), flags);
+          if (blocked < 0) blocked = collide(G, T.own, xyz(lds(win.o[slot])), rd, window_start(G, win, slot), flags);
         }
         if (blocked) {
           code = kBlocked;
