@@ -189,9 +189,16 @@ __device__ __forceinline__ float bilinear_p(const DevReceiver& R, float X, float
          (1 - fx) * fy * sample_p(R, c0, r0 + 1) + fx * fy * sample_p(R, c0 + 1, r0 + 1);
 }
 
-// Contribution of one ray that hit the receiver in the forward.
-__device__ __forceinline__ void ray_adjoint(const DevTask& T, const DiffTask& DT, const DevReceiver& R, int f, int lab,
-                                            float g[K]) {
+// What the rays of one facet share: its origin and the frame of its normal
+// (the slope-error perturbation's frame), as functions of the heliostat's
+// parameters, and its two pool offsets.
+struct FacetDual {
+  Dual3 origin;
+  DFrame pframe;
+  int g0, g1;
+};
+
+__device__ __forceinline__ FacetDual facet_dual(const DevTask& T, const DiffTask& DT, int f) {
   float3 local, ln;
   const bool focus_flat = facet_local(T, f, local, ln);
   DFrame hf;
@@ -199,12 +206,23 @@ __device__ __forceinline__ void ray_adjoint(const DevTask& T, const DiffTask& DT
   hf.n = DT.fn;
   hf.v = DT.v;
   hf.identity = DT.identity != 0;
-  const Dual3 origin = to_world(hf, local) + d3(T.pos);
+  FacetDual fd;
+  fd.origin = to_world(hf, local) + d3(T.pos);
   const Dual3 fnormal = focus_flat ? to_world(hf, ln) : DT.n;
-  const int g0 = __ldg(T.offsets + f), g1 = __ldg(T.offsets + (f + 1) % T.pool_size);
-  const float3 din = xyz(__ldg(T.samples + g0 + lab));
-  const float3 pert = xyz(__ldg(T.perturbations + g1 + lab));
-  const Dual3 np = normalize(to_world(make_dframe(fnormal, false), pert));
+  fd.pframe = make_dframe(fnormal, false);
+  fd.g0 = __ldg(T.offsets + f);
+  fd.g1 = __ldg(T.offsets + (f + 1) % T.pool_size);
+  return fd;
+}
+
+// Contribution of one ray (facet fd, light lab) that hit the receiver in the
+// forward.
+__device__ __forceinline__ void ray_adjoint(const DevTask& T, const DevReceiver& R, const FacetDual& fd, int lab,
+                                            float g[K]) {
+  const Dual3& origin = fd.origin;
+  const float3 din = xyz(__ldg(T.samples + fd.g0 + lab));
+  const float3 pert = xyz(__ldg(T.perturbations + fd.g1 + lab));
+  const Dual3 np = normalize(to_world(fd.pframe, pert));
   const Dual3 in = d3(make_float3(-din.x, -din.y, -din.z));
   const Dual3 rd = normalize(in - np * (dot(np, in) * 2.0f));
   const float3 o = val(origin), d = val(rd);
@@ -333,8 +351,43 @@ __device__ __forceinline__ void ray_adjoint(const DevTask& T, const DiffTask& DT
 }
 
 
-__global__ void __launch_bounds__(256) diff_backward_kernel(BackwardParams p) {
+// Facet window of the adjoint, per warp (as the trace kernel's): the
+// FacetDual of 32 consecutive facets, one per lane, stored component-major so
+// that lanes reading different slots touch different banks.
+constexpr int kBwdThreads = 128;
+constexpr int kDual3Words = 3 * (1 + K);
+struct AdjointWindow {
+  float origin[kDual3Words][kBwdThreads];
+  float frame[3 * kDual3Words][kBwdThreads];  // u, n, v
+  int g0[kBwdThreads], g1[kBwdThreads], identity[kBwdThreads];
+};
+
+__device__ __forceinline__ void put_dual3(float (*dst)[kBwdThreads], int slot, const Dual3& a) {
+  const Dual* c[3] = {&a.x, &a.y, &a.z};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    dst[i * (1 + K)][slot] = c[i]->v;
+#pragma unroll
+    for (int k = 0; k < K; ++k) dst[i * (1 + K) + 1 + k][slot] = c[i]->d[k];
+  }
+}
+
+__device__ __forceinline__ Dual3 get_dual3(const float (*src)[kBwdThreads], int slot) {
+  Dual3 a;
+  Dual* c[3] = {&a.x, &a.y, &a.z};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    c[i]->v = src[i * (1 + K)][slot];
+#pragma unroll
+    for (int k = 0; k < K; ++k) c[i]->d[k] = src[i * (1 + K) + 1 + k][slot];
+  }
+  return a;
+}
+
+__global__ void __launch_bounds__(kBwdThreads) diff_backward_kernel(BackwardParams p) {
+  __shared__ AdjointWindow win;
   const int lane = threadIdx.x & 31;
+  const int wbase = threadIdx.x & ~31;
   const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const long long chunk = p.chunk_begin + warp;
   if (chunk >= p.total_chunks) return;
@@ -351,9 +404,45 @@ __global__ void __launch_bounds__(256) diff_backward_kernel(BackwardParams p) {
   float g[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) g[k] = 0.0f;
+  int base = 0;
+  bool filled = false;  // warp-uniform
   for (int it = 0; it < iters; ++it) {
+    const bool active = r0 + it * 32 + lane < r_end;
     const unsigned bits = __ldg(p.hit_bits + warp * kChunkIters + it);
-    if ((bits >> lane) & 1u) ray_adjoint(T, DT, R, f, p.light_begin + l, g);
+    // The facets of an iteration lie within 32 of lane 0's (see the trace
+    // kernel); refill the window when a lane with a hit needs one past it.
+    const int f0 = __shfl_sync(0xffffffffu, f, 0);
+    const bool hit = active && ((bits >> lane) & 1u);
+    if (__any_sync(0xffffffffu, hit && (!filled || f - base >= 32))) {
+      __syncwarp();
+      base = f0;
+      filled = true;
+      const int fw = base + lane;
+      if (fw < T.num_facets) {
+        const FacetDual fd = facet_dual(T, DT, fw);
+        const int slot = wbase + lane;
+        put_dual3(win.origin, slot, fd.origin);
+        put_dual3(win.frame, slot, fd.pframe.u);
+        put_dual3(win.frame + kDual3Words, slot, fd.pframe.n);
+        put_dual3(win.frame + 2 * kDual3Words, slot, fd.pframe.v);
+        win.g0[slot] = fd.g0;
+        win.g1[slot] = fd.g1;
+        win.identity[slot] = fd.pframe.identity ? 1 : 0;
+      }
+      __syncwarp();
+    }
+    if (hit) {
+      const int slot = wbase + (f - base);
+      FacetDual fd;
+      fd.origin = get_dual3(win.origin, slot);
+      fd.pframe.u = get_dual3(win.frame, slot);
+      fd.pframe.n = get_dual3(win.frame + kDual3Words, slot);
+      fd.pframe.v = get_dual3(win.frame + 2 * kDual3Words, slot);
+      fd.pframe.identity = win.identity[slot] != 0;
+      fd.g0 = win.g0[slot];
+      fd.g1 = win.g1[slot];
+      ray_adjoint(T, R, fd, p.light_begin + l, g);
+    }
     f += p.lights_q32;
     l += p.lights_r32;
     if (l >= nl) {
@@ -434,9 +523,10 @@ cudaError_t launch_diff_backward(const BackwardParams& params, cudaStream_t stre
   BackwardParams p = params;
   p.lights_q32 = (int)(32 / nl);
   p.lights_r32 = (int)(32 % nl);
-  const long long blocks = (p.total_chunks - p.chunk_begin + 7) / 8;
+  const long long warps_per_block = kBwdThreads / 32;
+  const long long blocks = (p.total_chunks - p.chunk_begin + warps_per_block - 1) / warps_per_block;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-  diff_backward_kernel<<<(unsigned)blocks, 256, 0, stream>>>(p);
+  diff_backward_kernel<<<(unsigned)blocks, kBwdThreads, 0, stream>>>(p);
   return cudaGetLastError();
 }
 

@@ -389,3 +389,38 @@ def test_cpp_facade_traces_like_the_python_binding(tmp_path, cuda_device):
     assert want > 0
     assert float(res["image_sum"]) == pytest.approx(want, rel=1e-5)
     assert (tmp_path / "facade_after_smooth.txt").exists() and float(res["saved_max"]) > 0
+
+
+@pytest.mark.parametrize("sun", [[0.2, -0.26, 0.94], [-0.9, -0.3, 0.3]])
+def test_production_candidate_decisions_at_low_suns(tmp_path, sun):
+    """The production build decides shadowing and blocking from the candidate
+    lists without a grid walk; at low suns (many shadowed and blocked rays)
+    its per-ray outcomes must still agree with the oracle on >= 99.99 % of
+    rays and on every shadow / block decision but for rounding-level edge
+    rays (<= 1e-4 of the rays)."""
+    import json
+    from pathlib import Path
+
+    f = synth.large_field(tmp_path, seed=6, num_heliostats=40, helio_pixel=0.25, receiver_pixel=0.05, groups=4,
+                          per_group=128)
+    c = Case(f, seed=9)
+    cfg = json.loads(Path(f.config).read_text())
+    c2 = tmp_path / "sun.json"
+    c2.write_text(json.dumps(dict(cfg, sun_dir=sun)))
+    o2 = oracle.OracleScene.from_files(f.scene, c2)
+    c.scene.set_sun(sun)
+    c.scene.set_math_mode(0)
+    codes_s, codes_b = c.scene.shadow_free(), c.scene.block_free(0)
+    assert (codes_s >= 2).any() or (codes_b >= 2).any(), "no candidate lists at this sun"
+    L = c.scene.lights_per_group
+    agree = total = walls = 0
+    for h in range(0, c.scene.num_heliostats, 3):
+        nf = c.scene.heliostat(h)["num_facets"]
+        got = c.scene.hit_records(h, 0, min(nf, 150), 0, L)
+        want = o2.trace([h], c.dirs, c.pert, c.offsets, record=(h, 0, min(nf, 150)), images=False)["records"]
+        agree += int(np.sum((got >= 0) == (want >= 0)))
+        walls += int(np.sum(((got == -1) != (want == -1)) | ((got == -2) != (want == -2))))
+        total += got.size
+    assert agree >= 0.9999 * total, f"hit decisions agree on {agree / total:.6f}"
+    assert walls <= 1e-4 * total, f"{walls} of {total} shadow/block decisions differ"
+    print("sun", sun, "rays", total, "hit agreement", agree / total, "shadow/block differences", walls)
