@@ -25,6 +25,10 @@ the direction of travel, -(cos e sin a, sin e, cos e cos a) for azimuth a
                 150-1800 m over +-70 degrees, cylinder receiver r = 10 m,
                 h = 20 m at 200 m, 0.05 m micro-facets (40,000 per
                 heliostat), 20 m grid cells, 0.05 m receiver pixels.
+  two_receiver_field  two towers, each with its receiver and its own grid:
+                flat heliostats on a rectangle receiver to the north,
+                focus-flat heliostats on a cylinder to the south (the
+                reference's multi-receiver, multi-grid scene layout).
 """
 from __future__ import annotations
 
@@ -239,3 +243,54 @@ def huge_field(out_dir, seed: int = 0, num_heliostats: int = 10_000, helio_pixel
               "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
     return _write(out_dir, "huge", recv, grid, ["gap\t0.000000\t0.000000", "matrix\t1\t1"], pos,
                   (10.0, 0.1, 10.0), config)
+
+
+def two_receiver_field(out_dir, seed: int = 0, helio_pixel: float = 0.25, receiver_pixel: float = 0.05,
+                       groups: int = 4, per_group: int = 128) -> SceneFiles:
+    """Two receivers, one grid each: 12 flat 5x5 m heliostats north of a
+    rectangle receiver at (0, 40, 0) facing north, 12 focus-flat 6x4 m (2x2)
+    heliostats south of a cylinder receiver (r 2 m, h 4 m) at (0, 40, -200)."""
+    out_dir = Path(out_dir)
+    out_dir.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    lines = ["# synthetic scene two receivers", "ground\t1024.000000\t1024.000000", "ngrid\t2", ""]
+    north = [[(c - 1.5) * 10.0 + rng.uniform(-0.5, 0.5), 3.0, 40.0 + r * 10.0 + rng.uniform(-0.5, 0.5)]
+             for r in range(3) for c in range(4)]
+    south = [[(c - 1.5) * 10.0 + rng.uniform(-0.5, 0.5), 3.0, -240.0 - r * 10.0 + rng.uniform(-0.5, 0.5)]
+             for r in range(3) for c in range(4)]
+    blocks = [
+        (["Recv\t0", "pos\t\t0.000000\t40.000000\t0.000000", "size\t6.000000\t5.000000\t0.100000",
+          "norm\t0.000000\t0.000000\t1.000000", "face\t0", "end"],
+         0, ["gap\t0.000000\t0.000000", "matrix\t1\t1"], north, (5.0, 0.1, 5.0)),
+        (["Recv\t1", "pos\t\t0.000000\t40.000000\t-200.000000", "size\t2.000000\t4.000000\t0.000000",
+          "norm\t0.000000\t1.000000\t0.000000", "face\t0", "end"],
+         1, ["gap\t0.000000\t0.000000", "matrix\t2\t2", "surface_property -1 -1 -1 -1 -1 -1"], south,
+         (6.0, 0.1, 4.0)),
+    ]
+    n_total = 0
+    for recv, htype, block, pos, size in blocks:
+        pos = np.array(pos)
+        lines += recv + [""]
+        x0 = float(np.floor(pos[:, 0].min() - 10.0))
+        z0 = float(np.floor(pos[:, 2].min() - 10.0))
+        sx = float(np.ceil(pos[:, 0].max() + 10.0 - x0))
+        sz = float(np.ceil(pos[:, 2].max() + 10.0 - z0))
+        lines += ["Grid\t0", f"pos\t\t{_fmt(x0)}\t0.000000\t{_fmt(z0)}", f"size\t{_fmt(sx)}\t10.000000\t{_fmt(sz)}",
+                  "inter\t10.000000\t10.000000\t10.000000", f"n\t\t{len(pos)}", f"type\t{htype}", "end", ""]
+        lines += block
+        for p in pos:
+            lines.append("helio\t" + "\t".join(_fmt(v) for v in p))
+            lines.append("\t\t" + "\t".join(_fmt(v) for v in size))
+        lines.append("")
+        n_total += len(pos)
+    scene = out_dir / "two_scene.scn"
+    scene.write_text("\n".join(lines) + "\n")
+    config = {"sun_dir": sun_direction(150.0, 50.0), "dni": 1000.0, "csr": 0.1, "num_of_sunshape_groups": groups,
+              "num_per_sunshape_group": per_group, "inverse_transform_sampling_groups": 1024,
+              "receiver_pixel_length": receiver_pixel, "helio_disturb_std": 0.002,
+              "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
+    cfg = out_dir / "two_configuration.json"
+    cfg.write_text(json.dumps(config, indent=2) + "\n")
+    tasks = out_dir / "two_heliostat_index.txt"
+    tasks.write_text(f"{n_total}\n" + " ".join(str(i) for i in range(n_total)) + "\n")
+    return SceneFiles(scene, cfg, tasks, n_total)

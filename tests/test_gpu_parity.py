@@ -62,7 +62,13 @@ def large(tmp_path_factory, cuda_device):
     return Case(f)
 
 
-@pytest.fixture(params=["small", "large"])
+@pytest.fixture(scope="module")
+def two(tmp_path_factory, cuda_device):
+    # two receivers (rectangle, cylinder), each with its own grid
+    return Case(synth.two_receiver_field(tmp_path_factory.mktemp("two"), seed=3))
+
+
+@pytest.fixture(params=["small", "large", "two"])
 def case(request):
     return request.getfixturevalue(request.param)
 
