@@ -146,11 +146,36 @@ __device__ __forceinline__ bool box_meets(const float4* b, float3 o, float3 d) {
   return tn <= tf && tf >= -1.0f;
 }
 
+// Whether the ray hits the parallelogram (a, ab, ac): the reference's test
+// (rayParallelogramIntersect, Util/global_function.cuh:101-136), whose
+// blocker tests only use the answer.  The exact build divides as the
+// reference does.  The production builds compare the numerators against
+// |det| instead of dividing by det (u = nu / det lies in [0, 1] exactly when
+// nu * sign(det) lies in [0, |det|], and likewise v and t > 1e-5), which
+// answers the same except where a rounded quotient lands on a bound.
+__device__ __forceinline__ bool parallelogram_hit(float3 orig, float3 dir, float3 a, float3 ab, float3 ac) {
+#if defined(QM_TRACE_FAST_DIVIDE)
+  const float3 p = cross(dir, ac);
+  const float det = dot(ab, p);
+  if (qm_below_eps(fabsf(det))) return false;
+  const float sg = det > 0.0f ? 1.0f : -1.0f, ad = fabsf(det);
+  const float3 tv = sub(orig, a);
+  const float nu = dot(tv, p) * sg;
+  if (nu < 0.0f || nu > ad) return false;
+  const float3 q = cross(tv, ab);
+  const float nv = dot(dir, q) * sg;
+  if (nv < 0.0f || nv > ad) return false;
+  return dot(ac, q) * sg > 1.0e-5f * ad;
+#else
+  float t, u, v;
+  return ray_parallelogram(orig, dir, a, ab, ac, t, u, v);
+#endif
+}
+
 __device__ __forceinline__ bool sub_hit(const float4* sv, float3 o, float3 d) {
   float4 p0 = __ldg(sv), p1 = __ldg(sv + 1), p2 = __ldg(sv + 2);
-  float t, u, v;
-  return ray_parallelogram(o, d, make_float3(p0.x, p0.y, p0.z), make_float3(p0.w, p1.x, p1.y),
-                           make_float3(p1.z, p1.w, p2.x), t, u, v);
+  return parallelogram_hit(o, d, make_float3(p0.x, p0.y, p0.z), make_float3(p0.w, p1.x, p1.y),
+                           make_float3(p1.z, p1.w, p2.x));
 }
 
 // rectGridDDA::intersect over one cell (rectGridDDA.cu:7-25).  A heliostat
