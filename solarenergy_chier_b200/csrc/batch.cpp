@@ -236,6 +236,7 @@ int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scen
     b->d_verts.alloc(std::max<long long>(3 * n_sub, 1) * sizeof(float3));
     b->d_sub_free.alloc(std::max<long long>(n_sub, 1) * sizeof(int));
     b->d_sub_cand.alloc(std::max<long long>(n_sub, 1) * qm::kMaxCandidates * sizeof(int));
+    b->d_sub_frames.alloc(std::max<long long>(n_sub, 1) * 6 * sizeof(float4));
     b->d_images.alloc(std::max<long long>(n_img, 1) * sizeof(float));
     b->d_power.alloc(std::max(n_power, 1) * sizeof(double));
     b->d_pools.alloc(std::max<long long>(n_pool, 1) * sizeof(float4));
@@ -249,6 +250,7 @@ int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scen
       b->grids[g].subv = b->d_subv.as<float4>() + 3 * grid_slot[g].sub;
       b->grids[g].sub_free = b->d_sub_free.as<int>() + grid_slot[g].sub;
       b->grids[g].sub_cand = b->d_sub_cand.as<int>() + grid_slot[g].sub * qm::kMaxCandidates;
+      b->grids[g].sub_frames = b->d_sub_frames.as<float4>() + grid_slot[g].sub * 6;
     }
     for (size_t r = 0; r < b->receivers.size(); ++r) b->receivers[r].image = b->d_images.as<float>() + b->image_offset[r];
     for (const auto& I : b->inst)
@@ -262,6 +264,7 @@ int qmcrt_batch_create(qmcrt_scene* const* scenes, int n_scenes, const int* scen
       it.subv = b->d_subv.as<float4>() + 3 * sub;
       it.sub_free = b->d_sub_free.as<int>() + sub;
       it.sub_cand = b->d_sub_cand.as<int>() + sub * qm::kMaxCandidates;
+      it.sub_frames = b->d_sub_frames.as<float4>() + sub * 6;
       it.bound = b->d_bound.as<float4>() + gs.bound + 5 * item_slot[i].local;
       it.hsub = b->d_hsub.as<int4>() + gs.hsub + item_slot[i].local;
     }

@@ -24,7 +24,7 @@ struct qmcrt_batch {
   std::vector<qm::DevTask> tasks;
   std::vector<qm::PrepItem> items;
   qrt::DBuf d_grids, d_receivers, d_tasks, d_prefix, d_items, d_rot;
-  qrt::DBuf d_bound, d_hsub, d_subv, d_verts, d_sub_free, d_sub_cand;  // per instance-grid slices
+  qrt::DBuf d_bound, d_hsub, d_subv, d_verts, d_sub_free, d_sub_cand, d_sub_frames;  // per instance-grid slices
   qrt::DBuf d_images, d_power, d_diag, d_pools;
   int light_begin = 0, light_end = 0, max_lights = 0;
   long long total_chunks = -1;  // for the current light range; -1 = prefix not built
@@ -46,7 +46,7 @@ struct qmcrt_batch {
     cudaDeviceSynchronize();
     drop_graph();
     for (qrt::DBuf* b : {&d_grids, &d_receivers, &d_tasks, &d_prefix, &d_items, &d_rot, &d_bound, &d_hsub, &d_subv,
-                    &d_verts, &d_sub_free, &d_sub_cand, &d_images, &d_power, &d_diag, &d_pools})
+                    &d_verts, &d_sub_free, &d_sub_cand, &d_sub_frames, &d_images, &d_power, &d_diag, &d_pools})
       b->release();
     cudaSetDevice(prev);
   }

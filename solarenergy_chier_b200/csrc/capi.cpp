@@ -152,6 +152,8 @@ void build_device_scene(qmcrt_scene* s) {
     // block-free flags start cleared (no skipping) until the pools exist
     upload(gb->sub_free, std::vector<int>(std::max(g.num_subheliostats, 1), 0));
     upload(gb->sub_cand, std::vector<int>((size_t)std::max(g.num_subheliostats, 1) * qm::kMaxCandidates, -1));
+    gb->sub_frames.alloc((size_t)std::max(g.num_subheliostats, 1) * 6 * sizeof(float4));
+    cuda_check(cudaMemset(gb->sub_frames.p, 0, gb->sub_frames.bytes), "cudaMemset");
     DevGrid dg;
     dg.pos = g.pos;
     dg.interval = g.interval;
@@ -164,6 +166,7 @@ void build_device_scene(qmcrt_scene* s) {
     dg.subv = gb->subv.as<float4>();
     dg.sub_free = gb->sub_free.as<int>();
     dg.sub_cand = gb->sub_cand.as<int>();
+    dg.sub_frames = gb->sub_frames.as<float4>();
     s->grids.push_back(dg);
     s->grid_bufs.push_back(std::move(gb));
   }

@@ -30,6 +30,11 @@ struct DevGrid {
   // meeting none of their padded boxes skips the walk), 0 = walk.
   const int* sub_free;
   const int* sub_cand;
+  // Per sub-heliostat, for the tracer's facet window: the frame of its
+  // facets' world normal (u, n, v; identity flag in u.w) and, for focus-flat
+  // heliostats, the flipped frame of its local normal that places its facets
+  // (same layout): 6 float4, written with the walk codes for the current sun.
+  const float4* sub_frames;
 };
 
 struct DevReceiver {

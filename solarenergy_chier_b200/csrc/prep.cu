@@ -13,6 +13,7 @@
 #include "prep.h"
 
 #include "helio_geom.h"
+#include "ray_geom.h"
 #include "shadow.h"
 
 namespace qm {
@@ -94,6 +95,7 @@ __global__ void shadow_kernel(const PrepItem* items, int n, int max_sub, DevTask
   hf.v = T.fv;
   hf.identity = T.frame_identity != 0;
   const float3 nrm = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
+  sub_frames(T, s, it.sub_frames + 6 * s);
   const int k = it.block_theta >= 0.0f ? block_candidates(view, T.own, it.verts + 3 * s, it.sun_dir, nrm,
                                                          it.block_theta, it.sub_cand + kMaxCandidates * s,
                                                          kMaxCandidates)
@@ -129,6 +131,7 @@ __global__ void walk_flags_kernel(WalkFlagParams p) {
   hf.identity = T.frame_identity != 0;
   int* sub_free = const_cast<int*>(G.sub_free);
   int* sub_cand = const_cast<int*>(G.sub_cand);
+  sub_frames(T, s, const_cast<float4*>(G.sub_frames) + 6 * (hs.x + s));
   const float4* q = G.subv + 3 * (hs.x + s);
   const float3 A = make_float3(q[0].x, q[0].y, q[0].z);
   const float3 bac[3] = {make_float3(A.x + q[0].w, A.y + q[1].x, A.z + q[1].y), A,

@@ -31,6 +31,7 @@ struct PrepItem {
   float block_theta;
   int* sub_free;
   int* sub_cand;  // kMaxCandidates per sub-heliostat
+  float4* sub_frames;  // 6 per sub-heliostat (DevGrid::sub_frames)
   float3* verts;    // out: 3 float3 (B, A, C) per sub-heliostat
   float4* subv;     // out: 3 float4 per sub-heliostat (A, B - A, C - A)
   float4* bound;    // out: 5 float4 traversal record

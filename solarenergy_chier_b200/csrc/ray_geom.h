@@ -83,6 +83,67 @@ __device__ __forceinline__ bool facet_local(const DevTask& T, int f, float3& loc
   return true;
 }
 
+// Frames stored per sub-heliostat (DevGrid::sub_frames): 3 float4 (u, n, v;
+// identity flag in u.w).
+__device__ __forceinline__ void store_frame(float4* dst, const Frame& f) {
+  dst[0] = make_float4(f.u.x, f.u.y, f.u.z, f.identity ? 1.0f : 0.0f);
+  dst[1] = make_float4(f.n.x, f.n.y, f.n.z, 0.0f);
+  dst[2] = make_float4(f.v.x, f.v.y, f.v.z, 0.0f);
+}
+__device__ __forceinline__ Frame load_frame(const float4* src) {
+  const float4 u = __ldg(src), n = __ldg(src + 1), v = __ldg(src + 2);
+  Frame f;
+  f.u = make_float3(u.x, u.y, u.z);
+  f.n = make_float3(n.x, n.y, n.z);
+  f.v = make_float3(v.x, v.y, v.z);
+  f.identity = u.w != 0.0f;
+  return f;
+}
+
+// Both frames of sub-heliostat s of task T for the current sun: the frame
+// of its facets' world normal, as facet_geometry + qs::make_frame(normal,
+// false) form it, then the flipped frame of its local normal that
+// facet_local uses to place focus-flat facets.  Same operations, so the
+// tracer's facets are unchanged when it reads them instead.
+__device__ __forceinline__ void sub_frames(const DevTask& T, int s, float4* out) {
+  Frame hf;
+  hf.u = T.fu;
+  hf.n = T.fn;
+  hf.v = T.fv;
+  hf.identity = T.frame_identity != 0;
+  const float3 normal = T.type == 1 ? qs::to_world(hf, T.local_normals[s]) : T.normal;
+  store_frame(out, qs::make_frame(normal, false));
+  if (T.type == 1) store_frame(out + 3, qs::make_frame(T.local_normals[s], true));
+  else store_frame(out + 3, qs::make_frame(make_float3(0.f, 1.f, 0.f), true));
+}
+
+// Micro-facet f (of sub-heliostat `block`) in world space, with the frame of
+// its normal, from the sub-heliostat's stored frames (sf: its 6 float4):
+// facet_geometry + qs::make_frame without recomputing the per-sub-heliostat
+// frames.
+__device__ __forceinline__ void facet_geometry_framed(const DevTask& T, int f, int block, const float4* sf,
+                                                      float3& origin, Frame& normal_frame) {
+  Frame hf;
+  hf.u = T.fu;
+  hf.n = T.fn;
+  hf.v = T.fv;
+  hf.identity = T.frame_identity != 0;
+  float3 local, ln;
+  if (T.type == 0) {
+    facet_local(T, f, local, ln);
+  } else {
+    const int per_row = T.row_col.y * T.sub_row_col.y;
+    const int row = (f / per_row) % T.sub_row_col.x;
+    const int col = (f % per_row) % T.sub_row_col.y;
+    const float px = T.pixel_length;
+    const float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)col, 0.5f), px), T.sub_length.y / 2), 0.0f,
+                                  qm_rn_sub(qm_rn_mul(qm_rn_add((float)row, 0.5f), px), T.sub_length.x / 2));
+    local = qs::add(qs::to_world(load_frame(sf + 3), lp), T.local_centers[block]);
+  }
+  origin = qs::add(qs::to_world(hf, local), T.pos);
+  normal_frame = load_frame(sf);
+}
+
 // Micro-facet f in world space.
 __device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& origin, float3& normal) {
   Frame hf;

@@ -84,7 +84,7 @@ void upload(DBuf& b, const std::vector<T>& v) {
 }
 
 struct GridBufs {
-  DBuf ranges, entries, bound, hsub, subv, sub_free, sub_cand;
+  DBuf ranges, entries, bound, hsub, subv, sub_free, sub_cand, sub_frames;
 };
 
 class DeviceGuard {

@@ -486,18 +486,20 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
       filled = true;
       const int fw = base + lane;
       if (fw < T.num_facets) {
-        float3 origin, fnormal;
-        facet_geometry(T, fw, origin, fnormal);
-        const Frame fr = qs::make_frame(fnormal, false);
+        const int per_row = T.row_col.y * T.sub_row_col.y;
+        const int block = T.type == 1 ? (fw / per_row / T.sub_row_col.x) * T.row_col.y + (fw % per_row) / T.sub_row_col.y
+                                      : 0;
+        const int sub = __ldg(&G.hsub[T.own].x) + block;
+        // The facet and the frame of its normal, from its sub-heliostat's
+        // frames (computed once per sun with the walk codes).
+        float3 origin;
+        Frame fr;
+        facet_geometry_framed(T, fw, block, G.sub_frames + 6 * sub, origin, fr);
         win.o[wbase + lane] = make_float4(origin.x, origin.y, origin.z, __int_as_float(__ldg(T.offsets + fw)));
         // Pool offsets lie below 2^30; bit 31 carries the facet's
         // sub-heliostat block-free flag, and the frame word below its
         // candidate blockers (qm::block_candidates): n.w = sub-heliostat << 4
         // | candidates << 1 | frame identity.
-        const int per_row = T.row_col.y * T.sub_row_col.y;
-        const int block = T.type == 1 ? (fw / per_row / T.sub_row_col.x) * T.row_col.y + (fw % per_row) / T.sub_row_col.y
-                                      : 0;
-        const int sub = __ldg(&G.hsub[T.own].x) + block;
         const int bcode = __ldg(G.sub_free + sub);
         const int free_bit = bcode == 1 ? (int)0x80000000 : 0;
         const int cands = bcode >= 2 ? bcode - 1 : 0;
