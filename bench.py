@@ -82,7 +82,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--exact", action="store_true", help="time the kernel build without FMA contraction")
-    p.add_argument("--mode", type=int, default=None, help="kernel build: 0 production, 1 exact, 2 production/48 regs")
+    p.add_argument("--mode", type=int, default=None, help="kernel build: 0 production, 1 exact, 2 production at 4 blocks/SM")
     p.add_argument("--heliostats", type=int, default=0, help="trace only N heliostats (profiling)")
     p.add_argument("--heliostat-stride", type=int, default=1,
                    help="with --heliostats: take every S-th heliostat, spreading the slice over the field")
@@ -547,7 +547,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": kernel_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "math_mode": {0: "fast", 1: "exact", 2: "fast-48reg"}[mode],
+                "math_mode": {0: "fast", 1: "exact", 2: "fast-64reg"}[mode],
                 "data": "synthetic (seeded large_field: 624 heliostats, 187.6M micro-facets)",
                 "config": {"workload": WORKLOAD, "global_batch": f"{total_facets * passes * world} rays/step",
                            "rays_per_step_per_gpu": total_facets * passes, "passes_per_step": passes,

@@ -28,7 +28,7 @@ struct qmcrt_batch {
   qrt::DBuf d_images, d_power, d_diag, d_pools;
   int light_begin = 0, light_end = 0, max_lights = 0;
   long long total_chunks = -1;  // for the current light range; -1 = prefix not built
-  int mode = 0;                 // 0 production, 1 exact, 2 production 48 registers
+  int mode = 0;                 // 0 production, 1 exact, 2 production at 64 registers
   uint32_t* hit_bits = nullptr;  // output of bilinear-deposit launches (owned by the caller)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;

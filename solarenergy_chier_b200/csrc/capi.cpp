@@ -774,7 +774,7 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* s, unsigned seed) {
 
 int qmcrt_set_math_mode(qmcrt_scene* s, int exact) {
   return guarded([&] {
-    if (exact < 0 || exact > 2) invalid("math mode must be 0 (production), 1 (exact) or 2 (production, 48 registers)");
+    if (exact < 0 || exact > 2) invalid("math mode must be 0 (production), 1 (exact) or 2 (production, 64 registers)");
     checked(s)->exact = exact;
   });
 }

@@ -13,7 +13,7 @@ namespace qm {
 // (TraceParams::records), 2 bilinear deposit plus hit bits (TraceParams::hit_bits).
 cudaError_t launch_trace_fast(const TraceParams& p, int out, cudaStream_t stream);
 cudaError_t launch_trace_exact(const TraceParams& p, int out, cudaStream_t stream);
-// Production build limited to 48 registers (five 256-thread blocks per SM).
+// Production build limited to 64 registers (four 256-thread blocks per SM).
 cudaError_t launch_trace_fast4(const TraceParams& p, int out, cudaStream_t stream);
 // Rays per warp chunk; TraceParams::facet_prefix counts chunks per task.
 int trace_chunk_rays_fast();
