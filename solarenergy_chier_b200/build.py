@@ -40,7 +40,8 @@ CUDA_UNITS = [
                                        "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_fast4.o", ["-DQM_TRACE_VARIANT=fast4", "-DQM_TRACE_MIN_BLOCKS=4", "-DQM_TRACE_FAST_DIVIDE",
                                         "-DQM_TRACE_CANDIDATE_HITS"]),
-    ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-DQM_TRACE_MIN_BLOCKS=3", "-fmad=false"]),
+    ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-DQM_TRACE_THREADS=64", "-DQM_TRACE_MIN_BLOCKS=14",
+                                        "-fmad=false"]),
     ("pools.cu", "pools.o", []),
     # per-sun preparation: no FMA contraction, so it matches the host geometry bit for bit
     ("prep.cu", "prep.o", ["-fmad=false"]),

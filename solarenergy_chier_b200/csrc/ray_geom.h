@@ -117,28 +117,33 @@ __device__ __forceinline__ void sub_frames(const DevTask& T, int s, float4* out)
   else store_frame(out + 3, qs::make_frame(make_float3(0.f, 1.f, 0.f), true));
 }
 
-// Micro-facet f (of sub-heliostat `block`) in world space, with the frame of
-// its normal, from the sub-heliostat's stored frames (sf: its 6 float4):
-// facet_geometry + qs::make_frame without recomputing the per-sub-heliostat
-// frames.
-__device__ __forceinline__ void facet_geometry_framed(const DevTask& T, int f, int block, const float4* sf,
-                                                      float3& origin, Frame& normal_frame) {
+// Micro-facet at lattice row `row`, column `col` of its heliostat (facet
+// id = row * row_col.y * sub_row_col.y + col), in sub-heliostat lattice cell
+// (brow, bcol) = (row / sub_row_col.x, col / sub_row_col.y), in world
+// space, with the frame of its normal, from its sub-heliostat's stored
+// frames (sf: its 6 float4).  The same operations as facet_geometry +
+// qs::make_frame (facet_local's lattice arithmetic, its divisions done once
+// by the caller), without recomputing the per-sub-heliostat frames.
+__device__ __forceinline__ void facet_geometry_framed(const DevTask& T, int row, int col, int brow, int bcol,
+                                                      const float4* sf, float3& origin, Frame& normal_frame) {
   Frame hf;
   hf.u = T.fu;
   hf.n = T.fn;
   hf.v = T.fv;
   hf.identity = T.frame_identity != 0;
-  float3 local, ln;
+  const float px = T.pixel_length;
+  float3 local;
   if (T.type == 0) {
-    facet_local(T, f, local, ln);
+    local.x = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)col, px), qm_rn_mul((float)bcol, T.gap.x)), px / 2),
+                        T.size.x / 2);
+    local.y = T.size.y / 2;
+    local.z = qm_rn_sub(qm_rn_add(qm_rn_add(qm_rn_mul((float)row, px), qm_rn_mul((float)brow, T.gap.y)), px / 2),
+                        T.size.z / 2);
   } else {
-    const int per_row = T.row_col.y * T.sub_row_col.y;
-    const int row = (f / per_row) % T.sub_row_col.x;
-    const int col = (f % per_row) % T.sub_row_col.y;
-    const float px = T.pixel_length;
-    const float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)col, 0.5f), px), T.sub_length.y / 2), 0.0f,
-                                  qm_rn_sub(qm_rn_mul(qm_rn_add((float)row, 0.5f), px), T.sub_length.x / 2));
-    local = qs::add(qs::to_world(load_frame(sf + 3), lp), T.local_centers[block]);
+    const int lrow = row - brow * T.sub_row_col.x, lcol = col - bcol * T.sub_row_col.y;
+    const float3 lp = make_float3(qm_rn_sub(qm_rn_mul(qm_rn_add((float)lcol, 0.5f), px), T.sub_length.y / 2), 0.0f,
+                                  qm_rn_sub(qm_rn_mul(qm_rn_add((float)lrow, 0.5f), px), T.sub_length.x / 2));
+    local = qs::add(qs::to_world(load_frame(sf + 3), lp), T.local_centers[brow * T.row_col.y + bcol]);
   }
   origin = qs::add(qs::to_world(hf, local), T.pos);
   normal_frame = load_frame(sf);

@@ -486,15 +486,18 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
       filled = true;
       const int fw = base + lane;
       if (fw < T.num_facets) {
+        // Lattice position of the facet: row, column, and its sub-heliostat
+        // lattice cell (flat heliostats have one sub-heliostat).
         const int per_row = T.row_col.y * T.sub_row_col.y;
-        const int block = T.type == 1 ? (fw / per_row / T.sub_row_col.x) * T.row_col.y + (fw % per_row) / T.sub_row_col.y
-                                      : 0;
+        const int frow = fw / per_row, fcol = fw - frow * per_row;
+        const int brow = frow / T.sub_row_col.x, bcol = fcol / T.sub_row_col.y;
+        const int block = T.type == 1 ? brow * T.row_col.y + bcol : 0;
         const int sub = __ldg(&G.hsub[T.own].x) + block;
         // The facet and the frame of its normal, from its sub-heliostat's
         // frames (computed once per sun with the walk codes).
         float3 origin;
         Frame fr;
-        facet_geometry_framed(T, fw, block, G.sub_frames + 6 * sub, origin, fr);
+        facet_geometry_framed(T, frow, fcol, brow, bcol, G.sub_frames + 6 * sub, origin, fr);
         win.o[wbase + lane] = make_float4(origin.x, origin.y, origin.z, __int_as_float(__ldg(T.offsets + fw)));
         // Pool offsets lie below 2^30; bit 31 carries the facet's
         // sub-heliostat block-free flag, and the frame word below its
