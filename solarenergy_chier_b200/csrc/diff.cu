@@ -354,7 +354,13 @@ __device__ __forceinline__ void ray_adjoint(const DevTask& T, const DevReceiver&
 // Facet window of the adjoint, per warp (as the trace kernel's): the
 // FacetDual of 32 consecutive facets, one per lane, stored component-major so
 // that lanes reading different slots touch different banks.
-constexpr int kBwdThreads = 128;
+#ifndef QM_BWD_THREADS
+#define QM_BWD_THREADS 128
+#endif
+#ifndef QM_BWD_MIN_BLOCKS
+#define QM_BWD_MIN_BLOCKS 5
+#endif
+constexpr int kBwdThreads = QM_BWD_THREADS;
 constexpr int kDual3Words = 3 * (1 + K);
 struct AdjointWindow {
   float origin[kDual3Words][kBwdThreads];
@@ -384,7 +390,7 @@ __device__ __forceinline__ Dual3 get_dual3(const float (*src)[kBwdThreads], int 
   return a;
 }
 
-__global__ void __launch_bounds__(kBwdThreads) diff_backward_kernel(BackwardParams p) {
+__global__ void __launch_bounds__(kBwdThreads, QM_BWD_MIN_BLOCKS) diff_backward_kernel(BackwardParams p) {
   __shared__ AdjointWindow win;
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;
