@@ -36,11 +36,11 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xc
 
 HOST_SOURCES = ["scene.cpp", "buie_table.cpp", "capi.cpp", "batch.cpp", "diff.cpp", "pipeline.cpp"]
 CUDA_UNITS = [
-    ("tracer.cu", "tracer_fast.o", ["-DQM_TRACE_VARIANT=fast", "-DQM_TRACE_THREADS=64", "-DQM_TRACE_MIN_BLOCKS=14",
+    ("tracer.cu", "tracer_fast.o", ["-DQM_TRACE_VARIANT=fast", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
                                        "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_fast4.o", ["-DQM_TRACE_VARIANT=fast4", "-DQM_TRACE_MIN_BLOCKS=4", "-DQM_TRACE_FAST_DIVIDE",
                                         "-DQM_TRACE_CANDIDATE_HITS"]),
-    ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-DQM_TRACE_THREADS=64", "-DQM_TRACE_MIN_BLOCKS=14",
+    ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
                                         "-fmad=false"]),
     ("pools.cu", "pools.o", []),
     # per-sun preparation: no FMA contraction, so it matches the host geometry bit for bit

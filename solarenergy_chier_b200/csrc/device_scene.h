@@ -97,7 +97,7 @@ enum DiagSlot { kDiagClamped = 0, kDiagDdaCap = 1, kDiagSlots = 4 };
 // are one word per chunk iteration).  Larger chunks amortise the per-chunk
 // work (task lookup, facet window fill, power reduction) over more rays.
 #ifndef QM_CHUNK_ITERS
-#define QM_CHUNK_ITERS 32
+#define QM_CHUNK_ITERS 64
 #endif
 constexpr int kChunkIters = QM_CHUNK_ITERS;
 constexpr int kChunk = 32 * kChunkIters;

@@ -345,7 +345,7 @@ __device__ __forceinline__ bool collide(const DevGrid& g, int own, float3 o, flo
 // (at most ceil(32/nl) + 1 <= 32 of them), so a warp keeps a window of 32
 // facets in shared memory -- origin, normal frame and the two pool offsets --
 // computed one facet per lane, and refills it only when an iteration needs a
-// facet past its end (once per 32 facets: once per chunk of 1,024 rays at
+// facet past its end (once per 32 facets: twice per chunk of 2,048 rays at
 // 32 lights per facet).  Per-ray work then reads
 // the window instead of re-deriving the facet, and holds no facet state in
 // registers across the grid walks.
