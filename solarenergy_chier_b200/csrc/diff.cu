@@ -355,10 +355,10 @@ __device__ __forceinline__ void ray_adjoint(const DevTask& T, const DevReceiver&
 // FacetDual of 32 consecutive facets, one per lane, stored component-major so
 // that lanes reading different slots touch different banks.
 #ifndef QM_BWD_THREADS
-#define QM_BWD_THREADS 128
+#define QM_BWD_THREADS 32
 #endif
 #ifndef QM_BWD_MIN_BLOCKS
-#define QM_BWD_MIN_BLOCKS 5
+#define QM_BWD_MIN_BLOCKS 20
 #endif
 constexpr int kBwdThreads = QM_BWD_THREADS;
 constexpr int kDual3Words = 3 * (1 + K);
