@@ -113,6 +113,9 @@ __device__ __forceinline__ bool box_window(const float4* b, const int4* hs, floa
   const float olx = r.x * ax.x + r.y * ax.y + r.z * ax.z;
   const float dlx = d.x * ax.x + d.y * ax.y + d.z * ax.z;
   slab(olx, dlx, ax.w, tn, tf);
+  // Most rays miss here already (the thin plate's slab and one in-plane axis);
+  // a third slab can only narrow an empty interval further.
+  if (!(tn <= tf && tf >= -1.0f)) return false;
   const float4 az = __ldg(b + 3);
   const float olz = r.x * az.x + r.y * az.y + r.z * az.z;
   const float dlz = d.x * az.x + d.y * az.y + d.z * az.z;
