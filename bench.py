@@ -411,14 +411,18 @@ def run_reference(args):
         return
     times, rays_total = [], 0
     base = None
+    walls = []
     for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         b = cpu_baseline(files, max(2.0, 30.0 / max(args.steps, 1)))
         if step >= args.warmup:
             times.append(b)
+            walls.append(time.perf_counter() - t0)
         base = b
     value = statistics.mean(x["value"] for x in times)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 0,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(walls),
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded large_field)",
             "config": {"workload": WORKLOAD + " (reference per-ray routine on host cores)",
                        "global_batch": "sampled facets", "seq_len": None, "parallelism": "openmp"},
