@@ -430,3 +430,48 @@ def test_production_candidate_decisions_at_low_suns(tmp_path, sun):
     assert agree >= 0.9999 * total, f"hit decisions agree on {agree / total:.6f}"
     assert walls <= 1e-4 * total, f"{walls} of {total} shadow/block decisions differ"
     print("sun", sun, "rays", total, "hit agreement", agree / total, "shadow/block differences", walls)
+
+
+@pytest.mark.parametrize("lights", [(0, 1), (5, 8), (7, 40), (100, 137)])
+def test_ragged_light_ranges_match_oracle(small, lights):
+    """Light ranges that do not divide a warp (1, 3, 33 and 37 lights per
+    facet): the warp's lanes then span several facets and chunks end inside
+    a facet.  Exact build: per-ray outcomes identical to the oracle's and
+    FP64 powers equal to summation order (1e-9), for facet counts that are
+    not multiples of a chunk either."""
+    lb, le = lights
+    s = small.scene
+    s.set_math_mode(True)
+    ids = list(range(0, s.num_heliostats, 7))
+    for h in ids[:3]:
+        nf = s.heliostat(h)["num_facets"]
+        got = s.hit_records(h, 3, nf, lb, le)
+        want = small.o.trace([h], small.dirs, small.pert, small.offsets, light_begin=lb, light_end=le,
+                             record=(h, 3, nf), images=False)["records"]
+        assert np.array_equal(got, want), f"heliostat {h}, lights [{lb}, {le})"
+    small.reset()
+    s.set_light_range(lb, le)
+    s.trace(ids)
+    per, _ = s.power()
+    ref = small.o.trace(ids, small.dirs, small.pert, small.offsets, light_begin=lb, light_end=le)
+    np.testing.assert_allclose(per[ids], ref["power"][ids], rtol=1e-9, atol=0)
+    img = s.image(0).astype(np.float64)
+    assert np.abs(img - ref["images"][0]).sum() <= 1e-4 * max(ref["images"][0].sum(), 1e-30)
+    s.set_light_range(0, s.lights_per_group)
+    small.reset()
+
+
+def test_heliostats_without_micro_facets(tmp_path, cuda_device):
+    """Micro-facets larger than the heliostat (5 m facets on 4 m heliostats):
+    every heliostat has none, as the reference's int(length / pixel) gives;
+    tracing, batching and read-backs succeed with zero flux and power."""
+    f = synth.small_field(tmp_path, seed=1, helio_pixel=5.0, groups=4, per_group=128)
+    s = q.Scene(f.scene, f.config, device=0, seed=3)
+    assert all(s.heliostat(h)["num_facets"] == 0 for h in range(s.num_heliostats))
+    s.trace(list(range(s.num_heliostats)))
+    per, total = s.power()
+    assert total == 0.0 and not per.any() and not s.image(0).any()
+    assert s.hit_records(0, 0, 0, 0, s.lights_per_group).size == 0
+    b = q.Batch([s], [(0, [0.0, -0.866, -0.5])])
+    b.trace()
+    assert b.power(0)[1] == 0.0 and not b.image(0).any()
