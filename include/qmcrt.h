@@ -157,6 +157,18 @@ int qmcrt_power_clear(qmcrt_scene* scene);
  * [1] grid walks stopped by the step bound, [2..3] reserved. */
 int qmcrt_diagnostics(qmcrt_scene* scene, unsigned long long* out4);
 
+/* Rebuilds a grid's device cell lists on the GPU (count, scan, fill and
+ * sort kernels) instead of from the host's lists: the same lists as
+ * RectangleGrid::CGridHelioMatch builds (Scene/DataStructure/Grid/RectangleGrid.cu:62-117),
+ * every heliostat in every cell its box pos +- |size|/2 covers, in
+ * heliostat order.  The lists are replaced in place, so batches sharing
+ * them stay valid; call it with no trace of the scene in flight.  ms
+ * receives the device time of the build (may be NULL). */
+int qmcrt_grid_build_device(qmcrt_scene* scene, int grid, float* ms);
+/* Debug: the device cell lists of a grid: ranges (2 ints per cell,
+ * [begin, end)), entries (4 ints each: heliostat, first sub-heliostat,
+ * count, 0) and their number (either array may be NULL). */
+int qmcrt_debug_grid_cells(qmcrt_scene* scene, int grid, int* ranges, int* entries, long long* num_entries);
 /* Debug: per heliostat, the shadow-walk code for the current sun and pool:
  * 1 when the tracer skips its shadow walks because no other heliostat can
  * shadow any of its rays (a conservative capsule test around the sun-shape

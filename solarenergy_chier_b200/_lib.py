@@ -105,6 +105,8 @@ PROTOTYPES = {
     "qmcrt_diff_image": (_i, [_vp, _i, _pf, _pi, _pi]),
     "qmcrt_diff_power": (_i, [_vp, _pd, _pd]),
     "qmcrt_config_check": (_i, [ctypes.c_char_p, _pi]),
+    "qmcrt_grid_build_device": (_i, [_vp, _i, _pf]),
+    "qmcrt_debug_grid_cells": (_i, [_vp, _i, _pi, _pi, ctypes.POINTER(ctypes.c_longlong)]),
     "qmcrt_diff_create_suns": (_i, [_vp, _pf, _i, _f, ctypes.POINTER(_vp)]),
     "qmcrt_diff_set_hit_records": (_i, [_vp, _i, ctypes.c_longlong]),
     "qmcrt_diff_hit_records": (_i, [_vp, _pi, ctypes.POINTER(ctypes.c_longlong)]),

@@ -46,6 +46,7 @@ CUDA_UNITS = [
     # per-sun preparation: no FMA contraction, so it matches the host geometry bit for bit
     ("prep.cu", "prep.o", ["-fmad=false"]),
     ("diff.cu", "diff_kernels.o", []),
+    ("grid_build.cu", "grid_build.o", ["-fmad=false"]),
     ("smooth.cu", "smooth.o", []),
     ("microbench.cu", "microbench.o", []),
     ("smooth_static.cu", "smooth_static.o", []),

@@ -2,6 +2,7 @@
 #include "qmcrt.h"
 #include "helio_geom.h"
 #include "prep.h"
+#include "grid_build.h"
 
 #include <cuda_runtime.h>
 
@@ -883,6 +884,98 @@ int qmcrt_debug_shadow_free(qmcrt_scene* s, int* flags) {
     checked(s);
     if (!flags) invalid("output is NULL");
     for (size_t i = 0; i < s->templates.size(); ++i) flags[i] = s->templates[i].shadow_free;
+  });
+}
+
+int qmcrt_grid_build_device(qmcrt_scene* s, int grid, float* ms) {
+  return guarded([&] {
+    checked(s);
+    if (grid < 0 || grid >= (int)s->model.grids.size()) invalid("grid index out of range");
+    const qm::GridModel& g = s->model.grids[grid];
+    GridBufs& gb = *s->grid_bufs[grid];
+    DeviceGuard guard(s->device);
+    // Inputs: each heliostat's position and half size length (as the host
+    // grid builder forms them) and its sub-heliostat range.
+    std::vector<float4> pr(std::max(g.num_heliostats, 1));
+    std::vector<int2> subs(std::max(g.num_heliostats, 1));
+    for (int i = 0; i < g.num_heliostats; ++i) {
+      const qm::HeliostatModel& h = s->model.heliostats[g.start_heliostat + i];
+      const float radius = qm::length(h.size) / 2;
+      pr[i] = make_float4(h.pos.x, h.pos.y, h.pos.z, radius);
+      subs[i] = make_int2(h.sub_begin, h.num_sub);
+    }
+    const long long ncell = (long long)g.cells.x * g.cells.y * g.cells.z;
+    DBuf d_pr, d_subs, d_counts, d_ranges, d_total, d_entries;
+    upload(d_pr, pr);
+    upload(d_subs, subs);
+    d_counts.alloc((size_t)ncell * sizeof(int));
+    d_ranges.alloc((size_t)ncell * sizeof(int2));
+    d_total.alloc(sizeof(int));
+    qm::GridBuildParams p{};
+    p.pos = g.pos;
+    p.interval = g.interval;
+    p.cells = g.cells;
+    p.num_heliostats = g.num_heliostats;
+    p.pos_radius = d_pr.as<float4>();
+    p.subs = d_subs.as<int2>();
+    p.counts = d_counts.as<int>();
+    p.ranges = d_ranges.as<int2>();
+    p.total = d_total.as<int>();
+    cudaEvent_t e0, e1, e2;
+    cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&e2), "cudaEventCreate");
+    cuda_check(cudaEventRecord(e0, 0), "cudaEventRecord");
+    cuda_check(qm::launch_grid_count(p, 0), "grid count");
+    cuda_check(cudaEventRecord(e1, 0), "cudaEventRecord");
+    int total = 0;
+    cuda_check(cudaMemcpy(&total, d_total.p, sizeof(int), cudaMemcpyDeviceToHost), "grid total");
+    float t_count = 0.f, t_fill = 0.f;
+    cuda_check(cudaEventElapsedTime(&t_count, e0, e1), "cudaEventElapsedTime");
+    const size_t want = gb.entries.bytes / sizeof(int4);
+    if ((size_t)total != want) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      cudaEventDestroy(e2);
+      throw ApiError(QMCRT_ERR_INVALID, "device grid build found " + std::to_string(total) + " entries, the scene holds " +
+                                            std::to_string(want));
+    }
+    d_entries.alloc(std::max<size_t>(total, 1) * sizeof(int4));
+    p.entries = d_entries.as<int4>();
+    cuda_check(cudaEventRecord(e1, 0), "cudaEventRecord");
+    cuda_check(qm::launch_grid_fill(p, 0), "grid fill");
+    cuda_check(cudaEventRecord(e2, 0), "cudaEventRecord");
+    cuda_check(cudaEventSynchronize(e2), "grid build");
+    cuda_check(cudaEventElapsedTime(&t_fill, e1, e2), "cudaEventElapsedTime");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    // The scene's lists are replaced in place (same sizes), so batches that
+    // share them keep valid pointers.
+    cuda_check(cudaDeviceSynchronize(), "synchronise");
+    cuda_check(cudaMemcpy(gb.ranges.p, d_ranges.p, (size_t)ncell * sizeof(int2), cudaMemcpyDeviceToDevice),
+               "grid ranges");
+    if (total > 0)
+      cuda_check(cudaMemcpy(gb.entries.p, d_entries.p, (size_t)total * sizeof(int4), cudaMemcpyDeviceToDevice),
+                 "grid entries");
+    if (ms) *ms = t_count + t_fill;
+  });
+}
+
+int qmcrt_debug_grid_cells(qmcrt_scene* s, int grid, int* ranges, int* entries, long long* num_entries) {
+  return guarded([&] {
+    checked(s);
+    if (grid < 0 || grid >= (int)s->model.grids.size()) invalid("grid index out of range");
+    const qm::GridModel& g = s->model.grids[grid];
+    GridBufs& gb = *s->grid_bufs[grid];
+    const long long ncell = (long long)g.cells.x * g.cells.y * g.cells.z;
+    const long long n = (long long)(gb.entries.bytes / sizeof(int4));
+    if (num_entries) *num_entries = n;
+    DeviceGuard guard(s->device);
+    if (ranges)
+      cuda_check(cudaMemcpy(ranges, gb.ranges.p, (size_t)ncell * sizeof(int2), cudaMemcpyDeviceToHost), "readback");
+    if (entries && n > 0)
+      cuda_check(cudaMemcpy(entries, gb.entries.p, (size_t)n * sizeof(int4), cudaMemcpyDeviceToHost), "readback");
   });
 }
 

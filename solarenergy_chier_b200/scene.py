@@ -190,6 +190,23 @@ class Scene:
         check(self._lib.qmcrt_debug_block_free(self._h, grid, _ptr(f, ctypes.c_int)))
         return f
 
+    def build_grid_on_device(self, grid: int = 0) -> float:
+        """Rebuild the grid's device cell lists on the GPU; returns the build's device ms."""
+        ms = ctypes.c_float()
+        check(self._lib.qmcrt_grid_build_device(self._h, grid, ctypes.byref(ms)))
+        return ms.value
+
+    def device_grid_cells(self, grid: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """(ranges (cells, 2), entries (n, 4)) of the grid's device cell lists."""
+        n = ctypes.c_longlong()
+        check(self._lib.qmcrt_debug_grid_cells(self._h, grid, None, None, ctypes.byref(n)))
+        c = self.grid(grid)["cells"]
+        ranges = np.zeros((int(np.prod(c)), 2), np.int32)
+        entries = np.zeros((max(n.value, 1), 4), np.int32)
+        check(self._lib.qmcrt_debug_grid_cells(self._h, grid, _ptr(ranges, ctypes.c_int), _ptr(entries, ctypes.c_int),
+                                               ctypes.byref(n)))
+        return ranges, entries[:n.value]
+
     def set_sun(self, sun_dir) -> None:
         """Re-orient the field toward a new sun direction (direction of travel)."""
         d = np.ascontiguousarray(np.asarray(sun_dir, np.float32).reshape(3))
