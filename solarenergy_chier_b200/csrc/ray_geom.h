@@ -162,11 +162,23 @@ __device__ __forceinline__ void facet_geometry(const DevTask& T, int f, float3& 
   origin = qs::add(qs::to_world(hf, local), T.pos);
 }
 
+// The task of warp chunk w: the largest t with prefix[t] <= w.  Called by
+// all 32 lanes of a warp together: each round the lanes probe 32 points of
+// the remaining range at once and a ballot keeps the part holding the
+// answer, so the range shrinks 33-fold per round (4 rounds for 87,700 tasks
+// instead of 17 dependent halvings).
 __device__ __forceinline__ int find_task(const long long* prefix, int n, long long w) {
+  const int lane = threadIdx.x & 31;
   int lo = 0, hi = n - 1;
   while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
-    if (__ldg(prefix + mid) <= w) lo = mid; else hi = mid - 1;
+    const long long span = hi - lo;
+    const int probe = lo + (int)(((long long)(lane + 1) * span + 31) / 32);  // in (lo, hi], increasing
+    const unsigned below = __ballot_sync(0xffffffffu, __ldg(prefix + probe) <= w);
+    const int k = __popc(below);  // probes at or below w: lanes 0 .. k-1 (prefix is nondecreasing)
+    const int p_lo = __shfl_sync(0xffffffffu, probe, k > 0 ? k - 1 : 0);
+    const int p_hi = __shfl_sync(0xffffffffu, probe, k < 32 ? k : 31);
+    if (k > 0) lo = p_lo;
+    if (k < 32) hi = p_hi - 1;
   }
   return lo;
 }
