@@ -125,7 +125,7 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* scene, unsigned seed);
 
 /* exact = 1 selects the kernel build without FMA contraction (every float
  * operation rounded as the CPU oracle rounds it); 0 (default) the production
- * build (64-thread blocks, 72 registers per thread, 14 blocks per SM); 2
+ * build (one-warp blocks, 72 registers per thread, 28 blocks per SM); 2
  * the production build in 256-thread blocks at 64 registers (four per SM). */
 int qmcrt_set_math_mode(qmcrt_scene* scene, int exact);
 /* Trace only light indexes [begin, end) of every facet (default [0, per_group)).
