@@ -36,7 +36,15 @@ __device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, flo
   if (u < 0.0f || u > 1.0f) return false;
   float2 cs = qs::normalize2(make_float2(qm_rn_sub(ip.x, r.pos.x), qm_rn_sub(ip.z, r.pos.z)));
   float cx = fminf(fmaxf(cs.x, -1.0f), 1.0f);
+#if defined(QM_TRACE_FAST_DIVIDE)
+  // The double product with the reciprocal of 2 pi lies within one double
+  // ulp of the quotient, so the two round to different floats only when
+  // the quotient is within a double ulp of a float rounding boundary
+  // (about 2^-29 of rays).
+  v = (float)((double)acosf(cx) * (1.0 / (2 * M_PI)));
+#else
   v = (float)__ddiv_rn((double)acosf(cx), 2 * M_PI);
+#endif
   if (cs.y < 0) v = qm_rn_sub(1.0f, v);
   return true;
 }
