@@ -25,12 +25,25 @@ extern "C" {
 #define QMCRT_ERR_IO 2        /* unreadable or malformed file (reference: false + cerr)  */
 #define QMCRT_ERR_CUDA 3      /* CUDA runtime failure (reference: exit(1))               */
 #define QMCRT_ERR_STATE 4     /* call out of order, e.g. no sample pool yet              */
+#define QMCRT_ERR_NOMEM 5     /* device or host allocation failed (reference: exit(1))   */
 
 typedef struct qmcrt_scene qmcrt_scene;
 
 /* Message of the last failed call on this thread ("" when none). */
 const char* qmcrt_last_error(void);
 int qmcrt_version(void);
+
+/* Fault injection for callers' error paths.  The reference has no
+ * counterpart: it calls exit(1) when a CUDA allocation fails
+ * (Util/check_cuda.h:18-27).  Every allocation this library makes for a
+ * scene, batch or differentiable pair (device buffers, pinned staging, the
+ * scene state) passes one gate; after `after` more allocations succeed the
+ * next one fails with QMCRT_ERR_NOMEM and qmcrt_last_error() names it, as a
+ * real out-of-memory does, and the injection disarms itself.  after < 0
+ * disarms it.  The environment variable QMCRT_INJECT_ALLOC_FAILURE=<after>,
+ * read when the library loads, arms it for programs that cannot call this
+ * (e.g. bin/qmcrt).  Process-wide. */
+int qmcrt_debug_fail_allocations(long long after);
 
 /* ---- scene --------------------------------------------------------------
  * Replaces SceneConfiguration::getInstance()->loadConfiguration
@@ -191,6 +204,19 @@ int qmcrt_debug_block_free(qmcrt_scene* scene, int grid, int* flags);
 int qmcrt_debug_hit_records(qmcrt_scene* scene, int heliostat, int facet_begin, int facet_end,
                             int light_begin, int light_end, int* codes);
 
+/* Debug: one hit bit per ray of heliostats ids[0..n) over the scene's light
+ * range, traced by the current math mode with nothing deposited (no
+ * reference counterpart: the reference keeps no per-ray record).  Word w,
+ * bit i is ray (w / C) * 32 C + (w % C) * 32 + i of the launch's rays, with
+ * C = the tracer's warp-chunk iterations and rays numbered task by task, each
+ * task's rays padded to whole chunks of 32 C (facet-major, lights fastest);
+ * the layout depends only on the heliostat list and the light range, so two
+ * math modes' bit arrays compare ray by ray.  words receives the number of
+ * 32-bit words the launch needs; device_bits (device memory, capacity words;
+ * NULL = only report words) is cleared and filled. */
+int qmcrt_debug_hit_bits(qmcrt_scene* scene, const int* heliostats, int n, unsigned* device_bits,
+                         long long capacity, long long* words, void* stream);
+
 /* ---- batched tracing ------------------------------------------------------
  * No single reference counterpart: the reference traces one sun per
  * processed scene, one heliostat per QuasiMonteCarloRayTracer::rayTracing
@@ -300,7 +326,11 @@ int qmcrt_smooth(float* device_image, int width, int height, int radius, float t
  * library holds until exit; larger images fail with QMCRT_ERR_INVALID.  The
  * first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make it before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race. */
+ * capture.  The address is kept for the life of the process: after
+ * cudaDeviceReset (or any teardown of the device's primary context) the
+ * module is loaded again and the kept address is stale, so do not call this
+ * function on a device that has been reset.  All calls share the array:
+ * calls that overlap on the GPU race. */
 int qmcrt_smooth_static(float* device_image, int width, int height, int radius, float trim_ratio, void* stream);
 
 /* Replaces TaskLoader::loadRayTracingHeliostatIndex (RayTracingPipeline/TaskLoader.cpp:114-204).

@@ -27,6 +27,9 @@
 #include "SceneLoader.h"
 #include "SceneProcessor.h"
 #include "SolarScene.h"
+#include "Grid/rectGridDDA.cuh"
+#include "Receiver/receiverIntersectionUtil.cuh"
+#include "global_function.cuh"
 #undef private
 #undef protected
 
@@ -231,6 +234,131 @@ int refgpu_trace_with_offsets(int id, const int* offsets, int n_offsets) {
     cudaFree(verts);
     ha.CClear();
     return cudaGetLastError() == cudaSuccess ? 0 : -4;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+}  // extern "C"
+
+namespace {
+
+// Per-ray recorder of the reference's CUDA tracer: the steps of its
+// map_raytracing kernels (CylinderReceiverRectangleGridRayTracing.cu:6-40,
+// RectangleReceiverRectangleGridRayTracing.cu:6-41) for the rays of facets
+// [facet_begin, facet_end) x every light index, calling the reference's own
+// device functions (local2world_rotate, normalize, reflect,
+// rectGridDDA::collision, the receiver's GIntersect, calEnergy), with the
+// deposit (receiver_drawing's atomicAdd) replaced by a record per ray: the
+// outcome code (pixel index row * width + col as receiver_drawing computes
+// it, -1 shadowed, -2 blocked, -3 missed), u, v and the energy.
+template <class Recv>
+__global__ void record_rays(SunrayArgument sa, Recv recv, RectangleGrid grid, HeliostatArgument ha,
+                            float3* verts, float factor, int facet_begin, int facet_end, int* codes, float* u_out,
+                            float* v_out, float* energy) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int L = sa.numberOfLightsPerGroup;
+  if (i >= (long long)(facet_end - facet_begin) * L) return;
+  const long long ray = (long long)facet_begin * L + i;
+  const long long f = ray / L;
+  const int l = (int)(ray % L);
+  int address = (ha.d_microHelio_groups[f] + l) % sa.pool_size;
+  float3 dir = global_func::local2world_rotate(sa.d_samplelights[address], -sa.sunray_direction);
+  const float3 origin = ha.d_microHelio_origins[f];
+  int code = -1;
+  float t = 0.0f, u = 0.0f, v = 0.0f, e = 0.0f;
+  if (!rectGridDDA::collision(origin, dir, grid, verts, ha)) {
+    float3 normal = ha.d_microHelio_normals[f];
+    address = (ha.d_microHelio_groups[(f + 1) % sa.pool_size] + l) % sa.pool_size;
+    normal = global_func::local2world_rotate(sa.d_perturbations[address], normal);
+    normal = normalize(normal);
+    dir = normalize(reflect(-dir, normal));
+    if (rectGridDDA::collision(origin, dir, grid, verts, ha)) {
+      code = -2;
+    } else if (!recv.GIntersect(origin, dir, t, u, v)) {
+      code = -3;
+    } else {
+      e = calEnergy(t, dir, normal, factor);
+      const int2 res = recv.getResolution();
+      const int2 row_col = make_int2(u * res.y, v * res.x);
+      code = row_col.x * res.x + row_col.y;
+    }
+  }
+  codes[i] = code;
+  u_out[i] = u;
+  v_out[i] = v;
+  energy[i] = e;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Records every ray of facets [facet_begin, facet_end) of one heliostat
+// (all light indexes, row-major by facet) with the given facet offsets
+// (num_facets + 1 entries): host output arrays of (facet_end - facet_begin)
+// * lights entries each.  The reference's vertex table and micro-facets are
+// built by its own code, as refgpu_trace_with_offsets does.
+int refgpu_record_with_offsets(int id, const int* offsets, int n_offsets, int facet_begin, int facet_end,
+                               int* codes, float* u, float* v, float* energy) {
+  try {
+    SolarScene* s = SolarScene::GetInstance();
+    QuasiMonteCarloRayTracer tracer;
+    Sunray* sun = s->getSunray();
+    Heliostat* h = s->getHeliostats()[id];
+    Grid* grid = s->getGrids()[h->getBelongingGridId()];
+    Receiver* recv = s->getReceivers()[grid->getBelongingReceiverIndex()];
+    float3* verts = nullptr;
+    tracer.setFlatRectangleHeliostatVertexs(verts, s->getHeliostats(), grid->getStartHeliostatIndex(),
+                                            grid->getStartHeliostatIndex() + grid->getNumberOfHeliostats());
+    SunrayArgument sa = tracer.generateSunrayArgument(sun);
+    HeliostatArgument ha = tracer.generateHeliostatArgument(s, id);
+    if (n_offsets != ha.numberOfMicroHeliostats + 1 || facet_begin < 0 || facet_end > ha.numberOfMicroHeliostats ||
+        facet_begin >= facet_end) {
+      cudaFree(verts);
+      ha.CClear();
+      g_err = "offsets must hold num_facets + 1 entries and the facet range must lie inside the heliostat";
+      return -2;
+    }
+    cudaFree(ha.d_microHelio_groups);
+    ha.d_microHelio_groups = nullptr;
+    cudaMalloc(&ha.d_microHelio_groups, sizeof(int) * n_offsets);
+    cudaMemcpy(ha.d_microHelio_groups, offsets, sizeof(int) * n_offsets, cudaMemcpyHostToDevice);
+    float ratio = h->getPixelLength() / recv->getPixelLength();
+    float factor = sun->getDNI() * ratio * ratio * sun->getReflectiveRate() / float(sun->getNumOfSunshapeLightsPerGroup());
+    const long long n = (long long)(facet_end - facet_begin) * sa.numberOfLightsPerGroup;
+    int* d_codes = nullptr;
+    float *d_u = nullptr, *d_v = nullptr, *d_e = nullptr;
+    cudaMalloc(&d_codes, sizeof(int) * n);
+    cudaMalloc(&d_u, sizeof(float) * n);
+    cudaMalloc(&d_v, sizeof(float) * n);
+    cudaMalloc(&d_e, sizeof(float) * n);
+    const int threads = 256;
+    const unsigned blocks = (unsigned)((n + threads - 1) / threads);
+    if (recv->getType() == 0)
+      record_rays<<<blocks, threads>>>(sa, *dynamic_cast<RectangleReceiver*>(recv), *dynamic_cast<RectangleGrid*>(grid),
+                                       ha, verts, factor, facet_begin, facet_end, d_codes, d_u, d_v, d_e);
+    else
+      record_rays<<<blocks, threads>>>(sa, *dynamic_cast<CylinderReceiver*>(recv), *dynamic_cast<RectangleGrid*>(grid),
+                                       ha, verts, factor, facet_begin, facet_end, d_codes, d_u, d_v, d_e);
+    cudaError_t err = cudaDeviceSynchronize();
+    if (err == cudaSuccess) err = cudaGetLastError();
+    cudaMemcpy(codes, d_codes, sizeof(int) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(u, d_u, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(v, d_v, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(energy, d_e, sizeof(float) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d_codes);
+    cudaFree(d_u);
+    cudaFree(d_v);
+    cudaFree(d_e);
+    cudaFree(verts);
+    ha.CClear();
+    if (err != cudaSuccess) {
+      g_err = cudaGetErrorString(err);
+      return -4;
+    }
+    return 0;
   } catch (const std::exception& e) {
     g_err = e.what();
     return -1;

@@ -5,12 +5,15 @@ the reference tree by build_ref.py) with injected sample pools and facet
 offsets, in its own process (the reference keeps one scene per process in
 singletons), and saves its receiver images:
 
-    python -m oracle.ref_gpu_parity scene.scn config.json inputs.npz out.npz [per-heliostat]
+    python -m oracle.ref_gpu_parity scene.scn config.json inputs.npz out.npz [per-heliostat | record]
 
 inputs.npz: dirs (P, 3), pert (P, 3) float32 and, per traced heliostat h,
 offsets_<h> (num_facets + 1 int32).  out.npz: image<r> per receiver (all
 listed heliostats accumulated); with "per-heliostat", also image<r>_h<h>,
-each heliostat traced alone into a cleared image.
+each heliostat traced alone into a cleared image; with "record", also, per
+heliostat, every ray's outcome as the reference's kernel steps compute it
+(refgpu_record_with_offsets: code<h> int32 - pixel index, -1 shadowed,
+-2 blocked, -3 missed -, u<h>, v<h>, energy<h> float32, row-major by facet).
 """
 from __future__ import annotations
 
@@ -40,6 +43,9 @@ def main(argv) -> int:
     ok(L.refgpu_set_pools(dirs.ctypes.data_as(ctypes.c_void_p), pert.ctypes.data_as(ctypes.c_void_p),
                           dirs.shape[0]), "pools")
     per = len(argv) > 4 and argv[4] == "per-heliostat"
+    record = len(argv) > 4 and argv[4] == "record"
+    L.refgpu_num_facets.restype = ctypes.c_int
+    lights = L.refgpu_lights_per_group()
 
     def read(r):
         w, h = ctypes.c_int(), ctypes.c_int()
@@ -57,6 +63,15 @@ def main(argv) -> int:
         h = int(key.split("_")[1])
         o = np.ascontiguousarray(d[key], np.int32)
         ok(L.refgpu_trace_with_offsets(h, o.ctypes.data_as(ctypes.c_void_p), o.size), f"trace {h}")
+        if record:
+            n = (o.size - 1) * lights
+            rec = {"code": np.empty(n, np.int32), "u": np.empty(n, np.float32), "v": np.empty(n, np.float32),
+                   "energy": np.empty(n, np.float32)}
+            ok(L.refgpu_record_with_offsets(h, o.ctypes.data_as(ctypes.c_void_p), o.size, 0, o.size - 1,
+                                            *(rec[k].ctypes.data_as(ctypes.c_void_p)
+                                              for k in ("code", "u", "v", "energy"))), f"record {h}")
+            for k, a in rec.items():
+                images[f"{k}{h}"] = a
         if per:
             for r in range(counts[0]):
                 img = read(r)

@@ -12,7 +12,7 @@ PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libqmcrt.so"
 
 QMCRT_OK = 0
-ERRORS = {1: "invalid argument", 2: "I/O or format error", 3: "CUDA error", 4: "state error"}
+ERRORS = {1: "invalid argument", 2: "I/O or format error", 3: "CUDA error", 4: "state error", 5: "out of memory"}
 
 _i = ctypes.c_int
 _u = ctypes.c_uint
@@ -45,6 +45,7 @@ class QmcrtError(RuntimeError):
 PROTOTYPES = {
     "qmcrt_last_error": (ctypes.c_char_p, []),
     "qmcrt_version": (_i, []),
+    "qmcrt_debug_fail_allocations": (_i, [ctypes.c_longlong]),
     "qmcrt_scene_load": (_i, [ctypes.c_char_p, ctypes.c_char_p, _i, _u, ctypes.POINTER(_vp)]),
     "qmcrt_scene_free": (None, [_vp]),
     "qmcrt_scene_set_sun": (_i, [_vp, _pf]),
@@ -72,6 +73,7 @@ PROTOTYPES = {
     "qmcrt_power_clear": (_i, [_vp]),
     "qmcrt_diagnostics": (_i, [_vp, _pull]),
     "qmcrt_debug_hit_records": (_i, [_vp, _i, _i, _i, _i, _i, _pi]),
+    "qmcrt_debug_hit_bits": (_i, [_vp, _pi, _i, _vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong), _vp]),
     "qmcrt_debug_shadow_free": (_i, [_vp, _pi]),
     "qmcrt_debug_block_free": (_i, [_vp, _i, _pi]),
     "qmcrt_smooth": (_i, [_vp, _i, _i, _i, _f, _vp]),

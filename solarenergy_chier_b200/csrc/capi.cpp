@@ -7,7 +7,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -26,6 +28,12 @@
 
 namespace {
 thread_local std::string g_last_error;
+
+// Allocations left before an injected failure (< 0: injection off).
+std::atomic<long long> g_fail_after{[] {
+  const char* v = std::getenv("QMCRT_INJECT_ALLOC_FAILURE");
+  return v && *v ? std::atoll(v) : -1LL;
+}()};
 }  // namespace
 
 namespace qm {
@@ -35,6 +43,13 @@ void set_last_error(const std::string& msg) { g_last_error = msg; }
 using namespace qrt;
 
 namespace qrt {
+
+void alloc_gate(const char* what) {
+  long long left = g_fail_after.load();
+  while (left >= 0 && !g_fail_after.compare_exchange_weak(left, left - 1)) {
+  }
+  if (left == 0) throw ApiError(QMCRT_ERR_NOMEM, std::string(what) + ": injected allocation failure");
+}
 
 using qm::DevGrid;
 using qm::DevReceiver;
@@ -393,7 +408,9 @@ void ensure_stage(qmcrt_scene* s, size_t n) {
   s->h_stage = nullptr;
   s->h_prefix = nullptr;
   size_t cap = std::max<size_t>(n, 64);
+  alloc_gate("cudaMallocHost");
   cuda_check(cudaMallocHost((void**)&s->h_stage, cap * sizeof(DevTask)), "cudaMallocHost");
+  alloc_gate("cudaMallocHost");
   cuda_check(cudaMallocHost((void**)&s->h_prefix, (cap + 1) * sizeof(long long)), "cudaMallocHost");
   s->d_tasks.alloc(cap * sizeof(DevTask));
   s->d_prefix.alloc((cap + 1) * sizeof(long long));
@@ -412,24 +429,29 @@ qm::TraceParams base_params(qmcrt_scene* s) {
   return p;
 }
 
-cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st) {
+cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st) {
   switch (s->exact) {
-    case 1: return qm::launch_trace_exact(p, record, st);
-    case 2: return qm::launch_trace_fast4(p, record, st);
-    default: return qm::launch_trace_fast(p, record, st);
+    case 1: return qm::launch_trace_exact(p, out, st);
+    case 2: return qm::launch_trace_fast4(p, out, st);
+    default: return qm::launch_trace_fast(p, out, st);
   }
 }
 
-void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
+// Traces heliostats ids[0..n) over the scene's light range: out 0 adds their
+// flux and FP64 power, out 3 writes one hit bit per ray into hit_bits
+// (one 32-bit word per warp iteration of every warp chunk, chunks in task
+// order) and nothing else.  Returns the launch's number of warp chunks.
+long long trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream, int out = 0,
+                    uint32_t* hit_bits = nullptr) {
   if (n < 0 || (n > 0 && !ids)) invalid("heliostat list is invalid");
   for (int i = 0; i < n; ++i) check_heliostat(s, ids[i]);
-  if (n == 0) return;
+  if (n == 0) return 0;
   for (int i = 0; i < n; ++i)
     if ((long long)s->templates[ids[i]].num_facets * (s->light_end - s->light_begin) > kMaxTaskRays)
       invalid("a heliostat's micro-facets x lights must stay below 2^31 - 2^16 rays per launch; trace fewer lights");
   DeviceGuard guard(s->device);
   const long long nl = s->light_end - s->light_begin;
-  if (nl == 0) return;
+  if (nl == 0) return 0;
   const long long chunk = qm::trace_chunk_rays_fast();
   auto chunks_of = [&](int id) { return ((long long)s->templates[id].num_facets * nl + chunk - 1) / chunk; };
   bool same = s->cache_valid && s->cached_lights == nl && (int)s->cached_ids.size() == n &&
@@ -458,7 +480,10 @@ void trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream) {
   p.facet_prefix = s->d_prefix.as<long long>();
   p.num_tasks = n;
   p.total_facets = total;
-  cuda_check(run_trace(s, p, false, stream), "trace kernel");
+  p.hit_bits = hit_bits;
+  if (out == 3 && !hit_bits) return total;
+  cuda_check(run_trace(s, p, out, stream), "trace kernel");
+  return total;
 }
 
 int trace_chunk_rays() { return qm::trace_chunk_rays_fast(); }
@@ -468,6 +493,11 @@ int trace_chunk_rays() { return qm::trace_chunk_rays_fast(); }
 extern "C" {
 
 const char* qmcrt_last_error(void) { return g_last_error.c_str(); }
+
+int qmcrt_debug_fail_allocations(long long after) {
+  g_fail_after.store(after < 0 ? -1 : after);
+  return QMCRT_OK;
+}
 
 int qmcrt_version(void) { return 1; }
 
@@ -481,6 +511,7 @@ int qmcrt_scene_load(const char* scene_path, const char* config_path, int device
       cuda_check(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
       if (device >= ndev) invalid("device index out of range");
     }
+    alloc_gate("scene state");
     std::unique_ptr<qmcrt_scene> s(new qmcrt_scene());
     s->device = device;
     s->seed = seed;
@@ -798,6 +829,22 @@ int qmcrt_trace_heliostats(qmcrt_scene* s, const int* ids, int n, void* stream) 
   return guarded([&] { trace_ids(checked(s), ids, n, static_cast<cudaStream_t>(stream)); });
 }
 
+int qmcrt_debug_hit_bits(qmcrt_scene* s, const int* ids, int n, unsigned* device_bits, long long capacity,
+                         long long* words, void* stream) {
+  return guarded([&] {
+    checked(s);
+    if (capacity < 0) invalid("capacity must not be negative");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const long long need = trace_ids(s, ids, n, st, 3, nullptr) * qm::kChunkIters;
+    if (words) *words = need;
+    if (!device_bits) return;
+    if (capacity < need) invalid("the bit buffer holds fewer words than the launch needs");
+    DeviceGuard guard(s->device);
+    if (need > 0) cuda_check(cudaMemsetAsync(device_bits, 0, (size_t)need * sizeof(uint32_t), st), "clear bits");
+    trace_ids(s, ids, n, st, 3, reinterpret_cast<uint32_t*>(device_bits));
+  });
+}
+
 int qmcrt_receiver_image(qmcrt_scene* s, int id, float* out, int* width, int* height) {
   return guarded([&] {
     checked(s);
@@ -1028,7 +1075,7 @@ int qmcrt_debug_hit_records(qmcrt_scene* s, int id, int fb, int fe, int lb, int 
     p.record_task = 0;
     p.record_facet_begin = fb;
     p.record_facet_end = fe;
-    cuda_check(run_trace(s, p, true, 0), "record kernel");
+    cuda_check(run_trace(s, p, 1, 0), "record kernel");
     cuda_check(cudaMemcpy(codes, rec.p, count * sizeof(int32_t), cudaMemcpyDeviceToHost), "readback");
   });
 }
@@ -1042,6 +1089,7 @@ int qmcrt_smooth(float* d_img, int width, int height, int radius, float ratio, v
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t bytes = (size_t)width * height * sizeof(float);
     void* copy = nullptr;
+    alloc_gate("cudaMallocAsync");
     cuda_check(cudaMallocAsync(&copy, bytes, st), "cudaMallocAsync");
     cudaError_t e = cudaMemcpyAsync(copy, d_img, bytes, cudaMemcpyDeviceToDevice, st);
     if (e == cudaSuccess) e = qm::launch_trimmed_mean(static_cast<float*>(copy), d_img, width, height, radius, ratio, st);

@@ -26,8 +26,18 @@ struct ApiError : std::runtime_error {
 };
 
 inline void cuda_check(cudaError_t e, const char* what) {
+  if (e == cudaErrorMemoryAllocation) throw ApiError(QMCRT_ERR_NOMEM, std::string(what) + ": " + cudaGetErrorString(e));
   if (e != cudaSuccess) throw ApiError(QMCRT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
+
+// Allocation gate: every allocation the C ABI makes for a scene, batch or
+// differentiable pair (device buffers, pinned staging, the scene state
+// itself) passes here first.  When failure injection is armed
+// (QMCRT_INJECT_ALLOC_FAILURE=n in the environment when the library loads,
+// or qmcrt_debug_fail_allocations(n)), the allocation after n successful
+// ones fails with QMCRT_ERR_NOMEM as a real out-of-memory would, and
+// injection disarms itself.  Defined in capi.cpp.
+void alloc_gate(const char* what);
 
 // Runs one C ABI call: exceptions become status codes, their message the
 // thread's last error.
@@ -42,7 +52,7 @@ int guarded(F&& f) {
     return e.code;
   } catch (const std::bad_alloc&) {
     qm::set_last_error("host allocation failed");
-    return QMCRT_ERR_CUDA;
+    return QMCRT_ERR_NOMEM;
   } catch (const std::exception& e) {
     qm::set_last_error(e.what());
     return QMCRT_ERR_INVALID;
@@ -68,6 +78,7 @@ struct DBuf {
     if (n == bytes && p) return;
     release();
     if (n == 0) return;
+    alloc_gate("cudaMalloc");
     cuda_check(cudaMalloc(&p, n), "cudaMalloc");
     bytes = n;
   }
@@ -189,7 +200,8 @@ qmcrt_scene* checked(qmcrt_scene* s);
 // Sun axis and world-space tangent of the largest sun-shape angle for the
 // shadow-free test (tan_local < 0: unbounded, tan_world < 0).
 void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world);
-cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, bool record, cudaStream_t st);
+// out: 0 flux, 1 per-ray outcome codes, 3 hit bits (qm::TraceOut in tracer.cu).
+cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st);
 int trace_chunk_rays();
 constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;
 

@@ -10,7 +10,8 @@ namespace qm {
 // tracer.cu built with FMA contraction (production) and without it
 // (every float operation rounded as the CPU oracle rounds it).
 // out: 0 flux into the receiver images, 1 per-ray outcome codes
-// (TraceParams::records), 2 bilinear deposit plus hit bits (TraceParams::hit_bits).
+// (TraceParams::records), 2 bilinear deposit plus hit bits (TraceParams::hit_bits),
+// 3 hit bits alone.
 cudaError_t launch_trace_fast(const TraceParams& p, int out, cudaStream_t stream);
 cudaError_t launch_trace_exact(const TraceParams& p, int out, cudaStream_t stream);
 // Production build limited to 64 registers (four 256-thread blocks per SM).

@@ -259,6 +259,24 @@ class Scene:
                                                 _ptr(out, ctypes.c_int)))
         return out[:n]
 
+    def hit_bit_words(self, heliostats) -> int:
+        """32-bit words of the per-ray hit bits of `heliostats` over the light range."""
+        ids = np.ascontiguousarray(np.atleast_1d(np.asarray(heliostats, np.int32)))
+        words = ctypes.c_longlong()
+        check(self._lib.qmcrt_debug_hit_bits(self._h, _ptr(ids, ctypes.c_int), ids.size, None, 0,
+                                             ctypes.byref(words), None))
+        return words.value
+
+    def hit_bits(self, heliostats, device_ptr: int, capacity_words: int, stream=None) -> int:
+        """One hit bit per ray of `heliostats` (current light range and math
+        mode, nothing deposited) into `capacity_words` 32-bit words of device
+        memory at `device_ptr`; returns the words written."""
+        ids = np.ascontiguousarray(np.atleast_1d(np.asarray(heliostats, np.int32)))
+        words = ctypes.c_longlong()
+        check(self._lib.qmcrt_debug_hit_bits(self._h, _ptr(ids, ctypes.c_int), ids.size, ctypes.c_void_p(device_ptr),
+                                             capacity_words, ctypes.byref(words), _stream_handle(stream)))
+        return words.value
+
     def load_tasks(self, path) -> tuple[list, list, bool]:
         cap = self.num_heliostats + 1
         hs = np.zeros(cap, np.int32)

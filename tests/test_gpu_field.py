@@ -1,0 +1,149 @@
+"""Parity at the benchmark's own configuration (GPU, through the C ABI).
+
+The field bench.py times: 624 focus-flat heliostats (4x7 sub-heliostats,
+0.02 m micro-facets: 300,664 per heliostat, 187.6 M in all) at 100-750 m,
+cylinder receiver r 4 m x h 12 m (1257 x 600 pixels), Buie sun shape CSR 0.1
+from the 128 x 2048 pool, slope error 2.9 mrad, sun at azimuth 180 deg and
+elevation 60 deg, 20 m grid cells (synth.large_field(seed=0), the tracer's own
+pools and facet offsets, seed 0).
+
+Bars (the north star's, written here):
+  * per ray, on every 13th heliostat (48, spread over the field) x a 2,000-facet
+    range of each x all 2048 light indexes (197 M rays): the production
+    build's receiver-hit decisions agree with the host arithmetic (the CPU
+    oracle in float, which the reference's own host code pins bit for bit) on
+    >= 99.99 % of rays and its outcomes (pixel or miss code) on >= 99.9 %; the
+    exact build's outcomes are identical;
+  * the whole field for one bench step (light indexes 0-31, 6.0e9 rays): the
+    production build against the exact build -- which is the host arithmetic
+    ray for ray -- agrees on >= 99.99 % of all 6.0e9 hit decisions (one hit
+    bit per ray from each build), flux L1 <= 1e-3, total power <= 1e-5;
+  * FP64: on the same 48 heliostats x every facet x light indexes 0-7
+    (115 M rays) the production flux's L1 distance and total-power error
+    from the FP64 oracle are measured beside the host arithmetic's own; the
+    tracer may be no further from FP64 than the reference's float arithmetic
+    (1.05 x + 1e-4 in L1, + 2e-6 in power).
+"""
+import json
+
+import numpy as np
+import pytest
+
+import solarenergy_chier_b200 as q
+from oracle import oracle
+from solarenergy_chier_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+STRIDE = 13
+
+
+@pytest.fixture(scope="module")
+def field(tmp_path_factory, cuda_device):
+    files = synth.large_field(tmp_path_factory.mktemp("bench_field"), seed=0)
+    s = q.Scene(files.scene, files.config, device=0, seed=0)
+    dirs, pert = s.get_sample_pool()
+    ids = list(range(0, s.num_heliostats, STRIDE))
+    offsets = {h: s.get_facet_offsets(h) for h in ids}
+    yield files, s, dirs, pert, ids, offsets
+    s.close()
+
+
+def l1(a, b):
+    return float(np.abs(a - b).sum() / b.sum())
+
+
+def test_per_ray_outcomes_on_the_benchmark_field(field):
+    files, s, dirs, pert, ids, offsets = field
+    L = s.lights_per_group
+    assert s.num_heliostats == 624 and L == 2048 and s.pool_size == 128 * 2048
+    host = oracle.OracleScene.from_files(files.scene, files.config)
+    fp64 = oracle.OracleScene.from_files(files.scene, files.config, precision=64)
+    rng = np.random.default_rng(13)
+    n = prod_dec = prod_same = 0
+    prod_vs_fp64 = host_vs_fp64 = 0
+    for h in ids:
+        nf = s.heliostat(h)["num_facets"]
+        assert nf == 300664
+        fb = int(rng.integers(0, nf - 2000))
+        fe = fb + 2000
+        want = host.trace([h], dirs, pert, offsets, record=(h, fb, fe), images=False)["records"]
+        ref64 = fp64.trace([h], dirs, pert, offsets, record=(h, fb, fe), images=False)["records"]
+        s.set_math_mode(1)
+        exact = s.hit_records(h, fb, fe, 0, L)
+        assert np.array_equal(exact, want), f"heliostat {h}: exact build differs on {np.mean(exact != want):.2e}"
+        s.set_math_mode(0)
+        got = s.hit_records(h, fb, fe, 0, L)
+        n += got.size
+        prod_dec += int(np.count_nonzero((got >= 0) == (want >= 0)))
+        prod_same += int(np.count_nonzero(got == want))
+        prod_vs_fp64 += int(np.count_nonzero((got >= 0) != (ref64 >= 0)))
+        host_vs_fp64 += int(np.count_nonzero((want >= 0) != (ref64 >= 0)))
+    print("per-ray on the benchmark field:", json.dumps(
+        {"rays": n, "decision_agreement": prod_dec / n, "outcome_agreement": prod_same / n,
+         "decision_flips_vs_fp64": {"production": prod_vs_fp64 / n, "host_arithmetic": host_vs_fp64 / n}}))
+    assert prod_dec >= 0.9999 * n
+    assert prod_same >= 0.999 * n
+
+
+def test_whole_field_step_against_the_exact_build(field):
+    import torch
+
+    files, s, dirs, pert, _, _ = field
+    all_ids = list(range(s.num_heliostats))
+    s.set_light_range(0, 32)
+    words = s.hit_bit_words(all_ids)
+    rays = sum(s.heliostat(h)["num_facets"] for h in all_ids) * 32
+    assert words * 32 >= rays
+    bits = {}
+    results = {}
+    for mode in (1, 0):
+        s.set_math_mode(mode)
+        buf = torch.zeros(words, dtype=torch.int32, device="cuda")
+        s.hit_bits(all_ids, buf.data_ptr(), words)
+        torch.cuda.synchronize()
+        bits[mode] = buf
+        s.clear()
+        s.clear_power()
+        s.trace(all_ids)
+        results[mode] = (s.image(0).astype(np.float64), s.power()[1])
+    diff = torch.bitwise_xor(bits[0], bits[1])
+    nz = diff[diff != 0].cpu().numpy().view(np.uint8)
+    flips = int(np.unpackbits(nz).sum())
+    img0, p0 = results[0]
+    img1, p1 = results[1]
+    report = {"rays": rays, "decision_flips": flips, "decision_agreement": 1 - flips / rays,
+              "flux_l1": l1(img0, img1), "power_rel": abs(p0 - p1) / p1}
+    print("bench step, production vs exact build:", json.dumps(report))
+    s.set_light_range(0, s.lights_per_group)
+    assert flips <= 1e-4 * rays
+    assert report["flux_l1"] <= 1e-3
+    assert report["power_rel"] <= 1e-5
+
+
+def test_error_against_fp64_on_the_benchmark_field(field):
+    files, s, dirs, pert, ids, offsets = field
+    lights = 8
+    host = oracle.OracleScene.from_files(files.scene, files.config)
+    fp64 = oracle.OracleScene.from_files(files.scene, files.config, precision=64)
+    h32 = host.trace(ids, dirs, pert, offsets, 0, lights)
+    h64 = fp64.trace(ids, dirs, pert, offsets, 0, lights)
+    s.set_math_mode(0)
+    s.set_light_range(0, lights)
+    s.clear()
+    s.clear_power()
+    s.trace(ids)
+    img = s.image(0).astype(np.float64)
+    per, total = s.power()
+    s.set_light_range(0, s.lights_per_group)
+    ref32, ref64 = h32["images"][0], h64["images"][0]
+    t32, t64 = float(h32["power"].sum()), float(h64["power"].sum())
+    report = {"rays": h32["counters"]["rays"], "flux_l1_vs_fp64": l1(img, ref64),
+              "host_arithmetic_flux_l1_vs_fp64": l1(ref32, ref64), "flux_l1_vs_host_arithmetic": l1(img, ref32),
+              "power_rel_vs_fp64": abs(total - t64) / t64, "host_arithmetic_power_rel_vs_fp64": abs(t32 - t64) / t64,
+              "power_rel_vs_host_arithmetic": abs(total - t32) / t32}
+    print("FP64 on the benchmark field:", json.dumps(report))
+    assert report["flux_l1_vs_host_arithmetic"] <= 1e-3
+    assert report["power_rel_vs_host_arithmetic"] <= 1e-5
+    assert report["flux_l1_vs_fp64"] <= 1.05 * report["host_arithmetic_flux_l1_vs_fp64"] + 1e-4
+    assert report["power_rel_vs_fp64"] <= report["host_arithmetic_power_rel_vs_fp64"] + 2e-6

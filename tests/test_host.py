@@ -8,6 +8,7 @@ Tests/RayTracingPipelineTests/TaskLoaderTest.cpp).
 """
 import ctypes
 import json
+import os
 import re
 from pathlib import Path
 
@@ -19,7 +20,7 @@ from oracle import oracle, scene_text
 from solarenergy_chier_b200 import synth
 from tests.conftest import GOLDEN, ROOT
 
-REF = Path("/root/reference")
+REF = Path(os.environ.get("QMCRT_REFERENCE_TREE", "/root/reference"))
 GOOD_SCENE = """# Tests/DataStructureTests/test_file/test_scene_good.scn, restated
 ground 1024.000000 1024.000000
 ngrid 2
@@ -318,6 +319,48 @@ def test_errors_cross_the_boundary_as_codes(tmp_path):
     assert b"doesn't exist" in lib.qmcrt_last_error()
     assert lib.qmcrt_smooth(None, 4, 4, 1, 0.1, None) == 1
     assert lib.qmcrt_last_error() != b""
+
+
+def test_injected_allocation_failure_returns_a_status(tmp_path):
+    """An allocation that fails (here injected at the C ABI's allocation gate)
+    comes back as QMCRT_ERR_NOMEM with a message, where the reference calls
+    exit(1) (Util/check_cuda.h:18-27); the library stays usable after it."""
+    lib = q.load()
+    f = synth.small_field(tmp_path, seed=0, helio_pixel=0.5)
+    h = ctypes.c_void_p()
+    try:
+        assert lib.qmcrt_debug_fail_allocations(0) == 0
+        rc = lib.qmcrt_scene_load(str(f.scene).encode(), str(f.config).encode(), -1, 0, ctypes.byref(h))
+        assert rc == 5 and not h.value
+        assert lib.qmcrt_last_error() == b"scene state: injected allocation failure"
+        # injection disarmed itself: the same call now succeeds
+        assert lib.qmcrt_scene_load(str(f.scene).encode(), str(f.config).encode(), -1, 0, ctypes.byref(h)) == 0
+        lib.qmcrt_scene_free(h)
+        # a countdown: one allocation passes, then none is made by a host-only load
+        assert lib.qmcrt_debug_fail_allocations(1) == 0
+        assert lib.qmcrt_scene_load(str(f.scene).encode(), str(f.config).encode(), -1, 0, ctypes.byref(h)) == 0
+        lib.qmcrt_scene_free(h)
+        with pytest.raises(q.QmcrtError) as err:
+            q.Scene(f.scene, f.config, device=-1)
+        assert err.value.code == 5 and "injected allocation failure" in str(err.value)
+    finally:
+        lib.qmcrt_debug_fail_allocations(-1)
+
+
+def test_allocation_failure_injected_from_the_environment(tmp_path):
+    import subprocess
+    import sys
+
+    f = synth.small_field(tmp_path, seed=0, helio_pixel=0.5)
+    code = ("import ctypes, sys; lib = ctypes.CDLL(sys.argv[1]); h = ctypes.c_void_p(); "
+            "lib.qmcrt_last_error.restype = ctypes.c_char_p; "
+            "rc = lib.qmcrt_scene_load(sys.argv[2].encode(), sys.argv[3].encode(), -1, 0, ctypes.byref(h)); "
+            "print(rc, lib.qmcrt_last_error().decode())")
+    env = dict(os.environ, QMCRT_INJECT_ALLOC_FAILURE="0")
+    r = subprocess.run([sys.executable, "-c", code, str(q.LIB_PATH), str(f.scene), str(f.config)],
+                       capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "5 scene state: injected allocation failure"
 
 
 def test_pipeline_executable_rejects_bad_arguments(tmp_path):

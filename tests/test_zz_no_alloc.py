@@ -29,11 +29,13 @@ def _images(shape, seed):
     return img
 
 
-def _smooth(fn, img, radius, ratio):
+def _smooth(fn, img, radius, ratio, stream=None):
     import torch
 
     t = torch.from_numpy(img.copy()).cuda()
-    rc = fn(ctypes.c_void_p(t.data_ptr()), img.shape[1], img.shape[0], radius, ratio, None)
+    torch.cuda.synchronize()
+    handle = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+    rc = fn(ctypes.c_void_p(t.data_ptr()), img.shape[1], img.shape[0], radius, ratio, handle)
     torch.cuda.synchronize()
     return rc, t.cpu().numpy()
 
@@ -52,6 +54,31 @@ def test_static_smoother_matches_allocating_smoother_twice():
         assert rc_a == 0 and rc_b == 0, lib.qmcrt_last_error()
         # same kernel on the same copy: identical, well inside the smoother tests' tolerance
         assert np.array_equal(got, want)
+
+
+def test_static_smoother_with_large_heaps_on_a_side_stream():
+    """Radius 5 with trim ratio 0.25 needs 62 KiB of heaps per 256-thread
+    block, above the 48 KiB default (the launch raises the limit); the call
+    runs on a non-default stream, twice, and matches qmcrt_smooth.  A radius
+    whose heaps would need more than the 227 KiB a block can have is refused
+    with an error status instead of a launch, and the image is left as it was."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("needs a CUDA device")
+    lib = q.load()
+    side = torch.cuda.Stream()
+    for seed in (6, 7):
+        img = _images((211, 173), seed)
+        rc_a, want = _smooth(lib.qmcrt_smooth, img, 5, 0.25, side)
+        rc_b, got = _smooth(lib.qmcrt_smooth_static, img, 5, 0.25, side)
+        assert rc_a == 0 and rc_b == 0, lib.qmcrt_last_error()
+        assert np.array_equal(got, want)
+    img = _images((64, 64), 8)
+    rc, out = _smooth(lib.qmcrt_smooth_static, img, 10, 0.3)
+    assert rc == 3
+    assert lib.qmcrt_last_error().startswith(b"trimmed mean:")
+    assert np.array_equal(out, img)
 
 
 def test_static_smoother_allocates_nothing_and_rejects_large_images():
