@@ -139,7 +139,12 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* scene, unsigned seed);
 /* exact = 1 selects the kernel build without FMA contraction (every float
  * operation rounded as the CPU oracle rounds it); 0 (default) the production
  * build (one-warp blocks, 72 registers per thread, 28 blocks per SM); 2
- * the production build in 256-thread blocks at 64 registers (four per SM). */
+ * the production build in 256-thread blocks at 64 registers (four per SM);
+ * 3 the production build with approximate per-ray arithmetic after the
+ * shadow test (FMA contraction, hardware reciprocal square root and
+ * approximate divisions in the slope-error normal, reflection, receiver test
+ * and energy: hits near a pixel boundary or the cylinder's silhouette can
+ * land one pixel over or flip, as in the reference's own CUDA build). */
 int qmcrt_set_math_mode(qmcrt_scene* scene, int exact);
 /* Trace only light indexes [begin, end) of every facet (default [0, per_group)).
  * Energies keep the full-trace factor DNI*(hpx/rpx)^2*rho/per_group. */

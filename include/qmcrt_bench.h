@@ -14,6 +14,15 @@ extern "C" {
 int qmcrt_microbench_fp32(double* tflops);
 /* Float atomicAdd throughput into an n_pixels image at hashed addresses, 1e9/s. */
 int qmcrt_microbench_atomics(int n_pixels, double* giga_per_s);
+/* Replays recorded deposits: device_codes holds n_codes per-ray outcome
+ * codes in the tracer's lane order (pixel index >= 0 for a receiver hit, as
+ * qmcrt_debug_hit_records writes them); one launch adds 1.0f at every pixel
+ * code, `repeats` times over the list, 32 consecutive codes per warp.
+ * ms_per_launch receives the launch's device time (after a warm-up launch):
+ * hits x repeats / time is the L2 atomic rate of the tracer's own address
+ * pattern. */
+int qmcrt_microbench_atomics_replay(const int* device_codes, long long n_codes, int n_pixels, int repeats,
+                                    double* ms_per_launch);
 
 #ifdef __cplusplus
 }

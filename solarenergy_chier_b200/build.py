@@ -42,6 +42,8 @@ CUDA_UNITS = [
                                         "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
                                         "-fmad=false"]),
+    ("tracer.cu", "tracer_approx.o", ["-DQM_TRACE_VARIANT=approx", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
+                                         "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS", "-DQM_TRACE_APPROX_MATH"]),
     ("pools.cu", "pools.o", []),
     # per-sun preparation: no FMA contraction, so it matches the host geometry bit for bit
     ("prep.cu", "prep.o", ["-fmad=false"]),

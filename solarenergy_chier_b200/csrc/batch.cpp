@@ -131,11 +131,7 @@ cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chu
   p.power = b->d_power.as<double>();
   p.diag = b->d_diag.as<unsigned long long>();
   p.hit_bits = b->hit_bits;
-  switch (b->mode) {
-    case 1: return qm::launch_trace_exact(p, out, st);
-    case 2: return qm::launch_trace_fast4(p, out, st);
-    default: return qm::launch_trace_fast(p, out, st);
-  }
+  return launch_trace_mode(b->mode, p, out, st);
 }
 
 }  // namespace qrt
@@ -305,7 +301,7 @@ int qmcrt_batch_set_light_range(qmcrt_batch* b, int begin, int end) {
 int qmcrt_batch_set_math_mode(qmcrt_batch* b, int mode) {
   return guarded([&] {
     batch_checked(b);
-    if (mode < 0 || mode > 2) invalid("math mode must be 0, 1 or 2");
+    if (mode < 0 || mode > 3) invalid("math mode must be 0, 1, 2 or 3");
     b->mode = mode;
     b->drop_graph();
   });

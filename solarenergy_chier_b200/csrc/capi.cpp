@@ -429,12 +429,17 @@ qm::TraceParams base_params(qmcrt_scene* s) {
   return p;
 }
 
-cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st) {
-  switch (s->exact) {
+cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st) {
+  switch (mode) {
     case 1: return qm::launch_trace_exact(p, out, st);
     case 2: return qm::launch_trace_fast4(p, out, st);
+    case 3: return qm::launch_trace_approx(p, out, st);
     default: return qm::launch_trace_fast(p, out, st);
   }
+}
+
+cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st) {
+  return launch_trace_mode(s->exact, p, out, st);
 }
 
 // Traces heliostats ids[0..n) over the scene's light range: out 0 adds their
@@ -806,7 +811,8 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* s, unsigned seed) {
 
 int qmcrt_set_math_mode(qmcrt_scene* s, int exact) {
   return guarded([&] {
-    if (exact < 0 || exact > 2) invalid("math mode must be 0 (production), 1 (exact) or 2 (production, 64 registers)");
+    if (exact < 0 || exact > 3)
+      invalid("math mode must be 0 (production), 1 (exact), 2 (production, 64 registers) or 3 (approximate math)");
     checked(s)->exact = exact;
   });
 }

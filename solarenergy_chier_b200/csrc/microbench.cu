@@ -28,6 +28,23 @@ __global__ void atomic_kernel(float* img, int n_pix, int per_thread, uint32_t sa
   }
 }
 
+// Replays a recorded sequence of deposits: warp w of the grid takes groups
+// of 32 consecutive codes (one per lane, in the tracer's lane order) in a
+// grid-stride loop and adds 1 at every code >= 0 (a receiver pixel), as the
+// tracer's flux deposit does for the same rays.
+__global__ void replay_kernel(float* img, const int* __restrict__ codes, long long n_codes, int repeats) {
+  const long long lane = threadIdx.x & 31;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long groups = (n_codes + 31) >> 5;
+  for (int r = 0; r < repeats; ++r)
+    for (long long g = warp; g < groups; g += warps) {
+      const long long i = (g << 5) + lane;
+      const int code = i < n_codes ? __ldg(codes + i) : -1;
+      if (code >= 0) atomicAdd(img + code, 1.0f);
+    }
+}
+
 float time_launch(void (*launch)(void*), void* ctx) {
   cudaEvent_t a, b;
   cudaEventCreate(&a);
@@ -62,7 +79,34 @@ void atom_launch(void* p) {
   atomic_kernel<<<c->blocks, c->threads>>>(c->img, c->n_pix, c->per_thread, 17u);
 }
 
+struct ReplayCtx {
+  float* img;
+  const int* codes;
+  long long n_codes;
+  int blocks, threads, repeats;
+};
+void replay_launch(void* p) {
+  auto* c = static_cast<ReplayCtx*>(p);
+  replay_kernel<<<c->blocks, c->threads>>>(c->img, c->codes, c->n_codes, c->repeats);
+}
+
 }  // namespace
+
+extern "C" int qmcrt_microbench_atomics_replay(const int* device_codes, long long n_codes, int n_pixels, int repeats,
+                                               double* ms_per_launch) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (!device_codes || n_codes <= 0 || n_pixels <= 0 || repeats <= 0 || !ms_per_launch) return 1;
+  ReplayCtx c{nullptr, device_codes, n_codes, sms * 16, 256, repeats};
+  if (cudaMalloc(&c.img, sizeof(float) * n_pixels) != cudaSuccess) return 3;
+  cudaMemset(c.img, 0, sizeof(float) * n_pixels);
+  float ms = time_launch(replay_launch, &c);
+  cudaFree(c.img);
+  if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return 3;
+  *ms_per_launch = (double)ms;
+  return 0;
+}
 
 extern "C" int qmcrt_microbench_fp32(double* tflops) {
   int dev = 0, sms = 0;

@@ -54,6 +54,41 @@ __device__ __forceinline__ bool receiver_hit(const DevReceiver& r, float3 o, flo
   return cylinder_hit(r, o, d, t, u, v);
 }
 
+// The same cylinder test in approximate arithmetic (the approximate-math
+// tracer build): FMA contraction, the hardware reciprocal square root and
+// reciprocal-multiply divisions, v scaled by a float 1/(2 pi).  Rays near a
+// pixel boundary or at the cylinder's silhouette (where delta cancels) can
+// round to the neighbouring pixel or the other side of the silhouette; the
+// tracer's tests measure how many.
+__device__ __forceinline__ bool cylinder_hit_approx(const DevReceiver& r, float3 o, float3 d, float& t, float& u,
+                                                    float& v) {
+  const float lx = o.x - r.pos.x, lz = o.z - r.pos.z;
+  const float r2 = r.size.x * r.size.x;
+  if (lx * lx + lz * lz <= r2) return false;
+  const float dd = d.x * d.x + d.z * d.z;
+  const float il = rsqrtf(dd);
+  const float tp = -(lx * d.x + lz * d.z) * il;
+  const float delta = (lx * lx + lz * lz) - tp * tp;
+  if (qm_below_neg_eps(tp) || delta > r2) return false;
+  const float s = r2 - delta;
+  const float t_plus = delta <= 0.0f ? r.size.x : s * rsqrtf(s);
+  t = (tp - t_plus) * il;
+  const float3 ip = make_float3(d.x * t + o.x, d.y * t + o.y, d.z * t + o.z);
+  u = __fdividef(ip.y - r.pos.y, r.size.y) + 0.5f;
+  if (u < 0.0f || u > 1.0f) return false;
+  const float ex = ip.x - r.pos.x, ez = ip.z - r.pos.z;
+  const float cx = fminf(fmaxf(ex * rsqrtf(ex * ex + ez * ez), -1.0f), 1.0f);
+  v = acosf(cx) * 0.15915494f;
+  if (ez < 0) v = 1.0f - v;
+  return true;
+}
+
+__device__ __forceinline__ bool receiver_hit_approx(const DevReceiver& r, float3 o, float3 d, float& t, float& u,
+                                                    float& v) {
+  if (r.type == 0) return qf::ray_parallelogram(o, d, r.a, r.ab, r.ac, t, u, v);
+  return cylinder_hit_approx(r, o, d, t, u, v);
+}
+
 // Micro-facet centres and normals (rectangle_heliostat::map_microhelio_center_and_normal,
 // Scene/DataStructure/Heliostat/RectangleHelio.cu:54-80; focusFlatRectangle_heliostat
 // kernels, FocusFlatRectangleHelio.cu:12-64), evaluated per facet instead of

@@ -200,7 +200,9 @@ qmcrt_scene* checked(qmcrt_scene* s);
 // Sun axis and world-space tangent of the largest sun-shape angle for the
 // shadow-free test (tan_local < 0: unbounded, tan_world < 0).
 void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world);
-// out: 0 flux, 1 per-ray outcome codes, 3 hit bits (qm::TraceOut in tracer.cu).
+// out: 0 flux, 1 per-ray outcome codes, 2 bilinear deposit, 3 hit bits
+// (qm::TraceOut in tracer.cu); mode: the kernel build (qmcrt_set_math_mode).
+cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st);
 cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st);
 int trace_chunk_rays();
 constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;

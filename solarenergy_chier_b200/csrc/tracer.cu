@@ -20,10 +20,13 @@
 //
 // Everything outside the grid walk (sampling, facet geometry, slope error,
 // reflection, receiver intersection, energy) uses explicitly rounded
-// operations (qs::), so it rounds exactly as the CPU oracle does in both
-// builds.  The grid walk and its blocker tests (qm::) are compiled twice:
-// QM_TRACE_VARIANT=exact with -fmad=false, and QM_TRACE_VARIANT=fast with FMA
-// contraction (production).
+// operations (qs::), so it rounds exactly as the CPU oracle does.  The grid
+// walk and its blocker tests (qm::) are compiled with -fmad=false in the
+// exact build (QM_TRACE_VARIANT=exact) and with FMA contraction in the
+// production builds.  The approximate-math build (QM_TRACE_APPROX_MATH) also
+// evaluates the per-ray arithmetic after the shadow test with FMA
+// contraction, the hardware reciprocal square root and approximate
+// divisions (qf::); facet geometry stays explicitly rounded.
 #include <climits>
 
 #include "device_scene.h"
@@ -37,6 +40,20 @@
 #define QM_CAT2(a, b) a##_##b
 #define QM_CAT(a, b) QM_CAT2(a, b)
 #define QM_SYM(name) QM_CAT(name, QM_TRACE_VARIANT)
+
+// Per-ray arithmetic outside the walk (slope-error normal, reflection,
+// receiver test, energy, pixel index): explicitly rounded (qs::, as the CPU
+// oracle rounds it) in every build but the approximate-math one
+// (QM_TRACE_APPROX_MATH: qf::, FMA contraction and hardware approximations).
+#if defined(QM_TRACE_APPROX_MATH)
+namespace qx = ::qf;
+#define QM_RECEIVER_HIT receiver_hit_approx
+#define QM_PIXEL_MUL(a, b) ((a) * (b))
+#else
+namespace qx = ::qs;
+#define QM_RECEIVER_HIT receiver_hit
+#define QM_PIXEL_MUL(a, b) qm_rn_mul((a), (b))
+#endif
 
 namespace qm {
 namespace {
@@ -543,8 +560,8 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
         nframe.identity = (__float_as_int(wn.w) & 1) != 0;
         const int g1 = __float_as_int(lds(win.u[slot]).w);
         const int b = (g1 & 0x7fffffff) + lab;
-        float3 n = qs::normalize(qs::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
-        float3 rd = qs::normalize(qs::reflect(neg(dir), n));
+        float3 n = qx::normalize(qx::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
+        float3 rd = qx::normalize(qx::reflect(neg(dir), n));
         // Facets of sub-heliostats no other heliostat can block skip the
         // block walk; where only a few listed heliostats can
         // (qm::block_candidates, decided per sun with the pools),
@@ -560,19 +577,19 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
           code = kBlocked;
         } else {
           float tt, uu, vv;
-          if (!receiver_hit(R, xyz(lds(win.o[slot])), rd, tt, uu, vv)) {
+          if (!QM_RECEIVER_HIT(R, xyz(lds(win.o[slot])), rd, tt, uu, vv)) {
             code = kMissed;
           } else {
-            float e = qs::ray_energy(tt, rd, n, T.factor);
+            float e = qx::ray_energy(tt, rd, n, T.factor);
             if (kOut == kOutBits) {
               code = 0;
             } else if (kOut == kOutSplat) {
-              splat_bilinear(R, qm_rn_mul(vv, (float)R.resolution.x), qm_rn_mul(uu, (float)R.resolution.y), e);
+              splat_bilinear(R, QM_PIXEL_MUL(vv, (float)R.resolution.x), QM_PIXEL_MUL(uu, (float)R.resolution.y), e);
               power += (double)e;
               code = 0;
             } else {
-            int row = int(qm_rn_mul(uu, (float)R.resolution.y));
-            int col = int(qm_rn_mul(vv, (float)R.resolution.x));
+            int row = int(QM_PIXEL_MUL(uu, (float)R.resolution.y));
+            int col = int(QM_PIXEL_MUL(vv, (float)R.resolution.x));
             if (row >= R.resolution.y || col >= R.resolution.x || row < 0 || col < 0) {
               row = min(max(row, 0), R.resolution.y - 1);
               col = min(max(col, 0), R.resolution.x - 1);

@@ -16,6 +16,11 @@ cudaError_t launch_trace_fast(const TraceParams& p, int out, cudaStream_t stream
 cudaError_t launch_trace_exact(const TraceParams& p, int out, cudaStream_t stream);
 // Production build limited to 64 registers (four 256-thread blocks per SM).
 cudaError_t launch_trace_fast4(const TraceParams& p, int out, cudaStream_t stream);
+// Production build with approximate per-ray arithmetic after the shadow test
+// (FMA contraction, hardware reciprocal square root, approximate divisions).
+cudaError_t launch_trace_approx(const TraceParams& p, int out, cudaStream_t stream);
+int trace_chunk_rays_approx();
+cudaError_t launch_facets_approx(const DevTask& task, float3* origins, float3* normals, cudaStream_t stream);
 // Rays per warp chunk; TraceParams::facet_prefix counts chunks per task.
 int trace_chunk_rays_fast();
 int trace_chunk_rays_exact();

@@ -74,8 +74,35 @@ QM_HD float qm_rn_div(float a, float b) {
 #endif
 }
 
+// Correctly rounded reciprocal square root 1/sqrt(x): __frsqrt_rn on the
+// device; on the host evaluated in double and rounded once to float.
+QM_HD float qm_rn_rsqrt(float x) {
+#if defined(__CUDA_ARCH__)
+  return __frsqrt_rn(x);
+#else
+  return (float)(1.0 / sqrt((double)x));
+#endif
+}
+// Approximate forms (device: the hardware reciprocal square root and the
+// reciprocal-multiply division, within 2 ulp for the magnitudes the tracer
+// meets; host: the plain operations).
+QM_HD float qm_fast_rsqrt(float x) {
+#if defined(__CUDA_ARCH__)
+  return rsqrtf(x);
+#else
+  return (float)(1.0 / sqrt((double)x));
+#endif
+}
+QM_HD float qm_fast_div(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
+}
+
 // Orthonormal frame aligned with a normal: the columns (u, n, v) map local
-// (x, y, z) to world (shared by both variants below).
+// (x, y, z) to world (shared by the three variants below).
 namespace qm_frame {
 struct Frame {
   float3 u, n, v;
@@ -87,6 +114,7 @@ struct Frame {
 #define QS(a, b) ((a) - (b))
 #define QM(a, b) ((a) * (b))
 #define QD(a, b) ((a) / (b))
+#define QR(x) qm_rn_rsqrt(x)
 namespace qm {
 #include "vecmath_impl.h"
 }  // namespace qm
@@ -94,11 +122,13 @@ namespace qm {
 #undef QS
 #undef QM
 #undef QD
+#undef QR
 
 #define QA(a, b) qm_rn_add((a), (b))
 #define QS(a, b) qm_rn_sub((a), (b))
 #define QM(a, b) qm_rn_mul((a), (b))
 #define QD(a, b) qm_rn_div((a), (b))
+#define QR(x) qm_rn_rsqrt(x)
 namespace qs {
 using qm::kEps;
 #include "vecmath_impl.h"
@@ -107,3 +137,19 @@ using qm::kEps;
 #undef QS
 #undef QM
 #undef QD
+#undef QR
+
+#define QA(a, b) ((a) + (b))
+#define QS(a, b) ((a) - (b))
+#define QM(a, b) ((a) * (b))
+#define QD(a, b) qm_fast_div((a), (b))
+#define QR(x) qm_fast_rsqrt(x)
+namespace qf {
+using qm::kEps;
+#include "vecmath_impl.h"
+}  // namespace qf
+#undef QA
+#undef QS
+#undef QM
+#undef QD
+#undef QR

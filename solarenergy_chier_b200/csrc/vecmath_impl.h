@@ -1,8 +1,10 @@
-// Body of the float3 toolkit, included twice by vecmath.h: once with plain
-// operators (namespace qm: the compiler may contract a*b+c into an FMA) and
-// once with explicitly rounded operations (namespace qs: every multiply, add
-// and divide rounds separately, as in the CPU oracle, whatever the
-// compilation flags).  No include guard on purpose.
+// Body of the float3 toolkit, included three times by vecmath.h: with plain
+// operators (namespace qm: the compiler may contract a*b+c into an FMA),
+// with explicitly rounded operations (namespace qs: every multiply, add and
+// divide rounds separately, as in the CPU oracle, whatever the compilation
+// flags), and with plain operators plus the approximate reciprocal square
+// root and division (namespace qf, the approximate-math tracer build).  QR
+// is the reciprocal square root.  No include guard on purpose.
 
 
 
@@ -20,13 +22,7 @@ QM_HD float dot(float3 a, float3 b) { return QA(QA(QM(a.x, b.x), QM(a.y, b.y)), 
 QM_HD float3 cross(float3 a, float3 b) {
   return make_float3(QS(QM(a.y, b.z), QM(a.z, b.y)), QS(QM(a.z, b.x), QM(a.x, b.z)), QS(QM(a.x, b.y), QM(a.y, b.x)));
 }
-QM_HD float rlen(float d) {
-#if defined(__CUDA_ARCH__)
-  return __frsqrt_rn(d);
-#else
-  return (float)(1.0 / sqrt((double)d));
-#endif
-}
+QM_HD float rlen(float d) { return QR(d); }
 QM_HD float length(float3 v) { return sqrtf(dot(v, v)); }
 QM_HD float3 normalize(float3 v) { float inv = rlen(dot(v, v)); return mul(v, inv); }
 QM_HD float3 reflect(float3 i, float3 n) { return sub(i, mul(mul(n, 2.0f), dot(n, i))); }

@@ -24,3 +24,15 @@ def l2_atomics_per_s(n_pixels: int) -> float:
     out = ctypes.c_double()
     check(fn(int(n_pixels), ctypes.byref(out)))
     return out.value * 1e9
+
+
+def l2_atomics_replay_per_s(device_codes_ptr: int, n_codes: int, n_hits: int, n_pixels: int, repeats: int) -> float:
+    """Float atomics per second when the tracer's recorded deposits (device
+    array of n_codes outcome codes, n_hits of them pixels) are replayed."""
+    lib = load()
+    fn = lib.qmcrt_microbench_atomics_replay
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    ms = ctypes.c_double()
+    check(fn(ctypes.c_void_p(device_codes_ptr), int(n_codes), int(n_pixels), int(repeats), ctypes.byref(ms)))
+    return n_hits * repeats / (ms.value * 1e-3)

@@ -169,7 +169,8 @@ class Scene:
         check(self._lib.qmcrt_generate_facet_offsets(self._h, int(seed) & 0xFFFFFFFF))
 
     def set_math_mode(self, exact) -> None:
-        """True/1: exact build; False/0: production build; 2: production, 64 registers (4 blocks/SM)."""
+        """True/1: exact build; False/0: production build; 2: production, 64 registers (4 blocks/SM);
+        3: production with approximate per-ray arithmetic after the shadow test."""
         mode = int(exact) if not isinstance(exact, bool) else (1 if exact else 0)
         check(self._lib.qmcrt_set_math_mode(self._h, mode))
 

@@ -161,8 +161,10 @@ def radial_staggered(n: int, r_min: float, r_max: float, span_deg: float, seed: 
 
 def large_field(out_dir, seed: int = 0, num_heliostats: int = 624, helio_pixel: float = 0.02,
                 receiver_pixel: float = 0.02, groups: int = 128, per_group: int = 2048,
-                rows: int = 4, cols: int = 7) -> SceneFiles:
-    """The 624-heliostat focus-flat field with a cylinder receiver."""
+                rows: int = 4, cols: int = 7, keep_every: int = 1) -> SceneFiles:
+    """The 624-heliostat focus-flat field with a cylinder receiver
+    (keep_every = k keeps every k-th of its heliostats: a slice of the same
+    field, spread over it, with the same grid)."""
     xz = radial_staggered(num_heliostats, 100.0, 750.0, 70.0, seed)
     pos = np.stack([xz[:, 0], np.full(len(xz), 5.5), xz[:, 1]], axis=1)
     recv = ["Recv\t1", "pos\t\t0.000000\t115.000000\t0.000000", "size\t4.000000\t12.000000\t0.000000",
@@ -177,7 +179,7 @@ def large_field(out_dir, seed: int = 0, num_heliostats: int = 624, helio_pixel: 
               "receiver_pixel_length": receiver_pixel, "helio_disturb_std": 0.0029,
               "helio_pixel_length": helio_pixel, "helio_reflected_rate": 0.88}
     block = ["gap\t0.000000\t0.000000", f"matrix\t{rows}\t{cols}", "surface_property -1 -1 -1 -1 -1 -1"]
-    return _write(out_dir, "large", recv, grid, block, pos, (12.84, 0.1, 9.45), config)
+    return _write(out_dir, "large", recv, grid, block, pos[::keep_every], (12.84, 0.1, 9.45), config)
 
 
 def uneven_field(out_dir, index: int, seed: int = 0, helio_pixel: float = 0.05, receiver_pixel: float = 0.05,

@@ -18,6 +18,10 @@ Bars (the north star's, written here):
     production build against the exact build -- which is the host arithmetic
     ray for ray -- agrees on >= 99.99 % of all 6.0e9 hit decisions (one hit
     bit per ray from each build), flux L1 <= 1e-3, total power <= 1e-5;
+  * the approximate-math build (mode 3) meets the same per-ray decision and
+    whole-step bars; its outcomes (pixels) are reported, not bound: a hit
+    near a pixel boundary can land one pixel over, as in the reference's own
+    CUDA build (tests/test_gpu_reference.py);
   * FP64: on the same 48 heliostats x every facet x light indexes 0-7
     (115 M rays) the production flux's L1 distance and total-power error
     from the FP64 oracle are measured beside the host arithmetic's own; the
@@ -62,6 +66,7 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
     rng = np.random.default_rng(13)
     n = prod_dec = prod_same = 0
     prod_vs_fp64 = host_vs_fp64 = 0
+    approx_dec = approx_same = 0
     for h in ids:
         nf = s.heliostat(h)["num_facets"]
         assert nf == 300664
@@ -72,6 +77,10 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
         s.set_math_mode(1)
         exact = s.hit_records(h, fb, fe, 0, L)
         assert np.array_equal(exact, want), f"heliostat {h}: exact build differs on {np.mean(exact != want):.2e}"
+        s.set_math_mode(3)
+        approx = s.hit_records(h, fb, fe, 0, L)
+        approx_dec += int(np.count_nonzero((approx >= 0) == (want >= 0)))
+        approx_same += int(np.count_nonzero(approx == want))
         s.set_math_mode(0)
         got = s.hit_records(h, fb, fe, 0, L)
         n += got.size
@@ -81,12 +90,15 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
         host_vs_fp64 += int(np.count_nonzero((want >= 0) != (ref64 >= 0)))
     print("per-ray on the benchmark field:", json.dumps(
         {"rays": n, "decision_agreement": prod_dec / n, "outcome_agreement": prod_same / n,
+         "approx_math": {"decision_agreement": approx_dec / n, "outcome_agreement": approx_same / n},
          "decision_flips_vs_fp64": {"production": prod_vs_fp64 / n, "host_arithmetic": host_vs_fp64 / n}}))
     assert prod_dec >= 0.9999 * n
     assert prod_same >= 0.999 * n
+    assert approx_dec >= 0.9999 * n
 
 
-def test_whole_field_step_against_the_exact_build(field):
+@pytest.mark.parametrize("mode", [0, 3])
+def test_whole_field_step_against_the_exact_build(field, mode):
     import torch
 
     files, s, dirs, pert, _, _ = field
@@ -97,25 +109,26 @@ def test_whole_field_step_against_the_exact_build(field):
     assert words * 32 >= rays
     bits = {}
     results = {}
-    for mode in (1, 0):
-        s.set_math_mode(mode)
+    for m in (1, mode):
+        s.set_math_mode(m)
         buf = torch.zeros(words, dtype=torch.int32, device="cuda")
         s.hit_bits(all_ids, buf.data_ptr(), words)
         torch.cuda.synchronize()
-        bits[mode] = buf
+        bits[m] = buf
         s.clear()
         s.clear_power()
         s.trace(all_ids)
-        results[mode] = (s.image(0).astype(np.float64), s.power()[1])
-    diff = torch.bitwise_xor(bits[0], bits[1])
+        results[m] = (s.image(0).astype(np.float64), s.power()[1])
+    diff = torch.bitwise_xor(bits[mode], bits[1])
     nz = diff[diff != 0].cpu().numpy().view(np.uint8)
     flips = int(np.unpackbits(nz).sum())
-    img0, p0 = results[0]
+    img0, p0 = results[mode]
     img1, p1 = results[1]
     report = {"rays": rays, "decision_flips": flips, "decision_agreement": 1 - flips / rays,
               "flux_l1": l1(img0, img1), "power_rel": abs(p0 - p1) / p1}
-    print("bench step, production vs exact build:", json.dumps(report))
+    print(f"bench step, mode {mode} vs exact build:", json.dumps(report))
     s.set_light_range(0, s.lights_per_group)
+    s.set_math_mode(0)
     assert flips <= 1e-4 * rays
     assert report["flux_l1"] <= 1e-3
     assert report["power_rel"] <= 1e-5

@@ -1,0 +1,73 @@
+"""The drop-in executable end to end on the GPU, against the reference's own
+pipeline steps.
+
+bin/qmcrt -c config -s scene -h tasks -o out/ (RayTracingPipeline::rayTracing,
+RayTracingPipeline/RayTracingPipeline.cpp:16-142) traces every listed
+heliostat on the GPU (production build, seed-0 pools and facet offsets) and
+writes <receiver>_receiver_before_smooth.txt and _after_smooth.txt per
+receiver index of the task list.  oracle/ref_pipeline.py runs the same steps
+on the reference's own host code (its TaskLoader, per-ray routine, ImageSaver
+and trimmed-mean heaps) with the executable's pools and offsets, read back
+through the Python binding of the same seed.
+
+Bar (written here): the same files, and in each every value equal to the
+reference's to the format's two decimals, except where float accumulation
+order or a per-ray difference of the production build moves a value across
+a rounding boundary: at most one unit in the last place, on at most 1 % of
+the pixels, and the totals of each file within 1e-5.
+"""
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import solarenergy_chier_b200 as q
+from solarenergy_chier_b200 import synth
+from tests.conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+REF_HOST = ROOT / "oracle" / "_ref" / "libref_host.so"
+
+
+def read_csv(path):
+    rows = [line.strip() for line in path.read_text().splitlines() if line.strip()]
+    return np.array([[float(x) for x in row.rstrip(",").split(",")] for row in rows])
+
+
+@pytest.mark.skipif(not REF_HOST.exists(), reason="the reference's host library (oracle/_ref) is absent")
+@pytest.mark.parametrize("which", ["two_receivers", "flat_field"])
+def test_executable_writes_the_reference_pipeline_files(which, tmp_path, cuda_device):
+    if which == "two_receivers":
+        f = synth.two_receiver_field(tmp_path / "in", seed=3)
+    else:
+        f = synth.small_field(tmp_path / "in", seed=1, helio_pixel=0.2, groups=8, per_group=256)
+    ours, ref = tmp_path / "ours", tmp_path / "ref"
+    ours.mkdir()
+    ref.mkdir()
+    r = subprocess.run([str(q.executable()), "-c", str(f.config), "-s", str(f.scene), "-h", str(f.tasks),
+                        "-o", str(ours) + "/"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    s = q.Scene(f.scene, f.config, device=0, seed=0)  # the executable's seed: same pools and offsets
+    dirs, pert = s.get_sample_pool()
+    ids, _, _ = s.load_tasks(f.tasks)
+    np.savez(tmp_path / "inputs.npz", dirs=dirs, pert=pert, per_group=s.lights_per_group,
+             **{f"offsets_{h}": s.get_facet_offsets(h) for h in ids})
+    s.close()
+    r = subprocess.run([sys.executable, "-m", "oracle.ref_pipeline", str(f.config), str(f.scene), str(f.tasks),
+                        str(tmp_path / "inputs.npz"), str(ref)], cwd=str(ROOT), capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    names = sorted(p.name for p in ref.iterdir())
+    assert names and names == sorted(p.name for p in ours.iterdir())
+    for name in names:
+        a, b = read_csv(ours / name), read_csv(ref / name)
+        assert a.shape == b.shape, name
+        diff = np.abs(a - b)
+        frac = float(np.mean(diff > 1e-9))
+        print(f"{which} {name}: {a.shape}, max |diff| {diff.max():.3f}, differing values {frac:.2e}, "
+              f"total {a.sum():.2f} vs {b.sum():.2f}")
+        assert diff.max() <= 0.0100001, name
+        assert frac <= 0.01, name
+        assert abs(a.sum() - b.sum()) <= 1e-5 * max(b.sum(), 1.0) + 0.01 * diff.size * frac, name

@@ -83,14 +83,14 @@ def field(tmp_path_factory):
     return files, o, full, d
 
 
-def _run_ranks(files, split, out, world=2):
+def _run_ranks(files, split, out, world=2, argv=None):
     env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()), WORLD_SIZE=str(world),
                OMP_NUM_THREADS="2")
     procs = []
+    args = argv if argv is not None else [str(files.scene), str(files.config), split, str(LIGHTS), str(out)]
     for rank in range(world):
         e = dict(env, RANK=str(rank), LOCAL_RANK=str(rank))
-        procs.append(subprocess.Popen([sys.executable, str(ROOT / "tests" / "shard_worker.py"), str(files.scene),
-                                       str(files.config), split, str(LIGHTS), str(out)], env=e,
+        procs.append(subprocess.Popen([sys.executable, str(ROOT / "tests" / "shard_worker.py"), *args], env=e,
                                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT))
     logs = []
     for p in procs:
@@ -122,3 +122,51 @@ def test_light_split_reduces_to_the_one_rank_trace(field):
     assert float(r["total"]) == pytest.approx(float(full["power"].sum()), rel=1e-12)
     for k in range(o.num_receivers):
         np.testing.assert_allclose(r[f"image{k}"], full["images"][k], rtol=1e-12, atol=1e-9)
+
+
+def test_instance_shards_cover_and_balance():
+    rays = [5, 9, 1, 7, 7, 3]
+    sh = shard.instance_shards(rays, 2)
+    assert sorted(k for ids in sh for k in ids) == list(range(6))
+    loads = [sum(rays[k] for k in ids) for ids in sh]
+    assert abs(loads[0] - loads[1]) <= max(rays)
+    assert shard.sun_shards(32, 3) == [(0, 11), (11, 22), (22, 32)]
+
+
+def test_batch_split_gathers_every_instance(field, tmp_path):
+    """Instances (the field at 6 suns) split over two gloo ranks by
+    ShardedBatch, each rank tracing its own with the CPU oracle: rank 0
+    receives every instance, each equal to a one-rank trace of it."""
+    from solarenergy_chier_b200 import synth as sy
+    from tests.shard_models import OracleBatch
+
+    files, o, full, d = field
+    r = _run_ranks(files, None, tmp_path / "b.npz", argv=["batch", str(files.scene), str(files.config),
+                                                           str(tmp_path / "b.npz")])
+    suns = sy.sun_positions(days=2, hours=3)
+    assert int(r["n"]) == len(suns)
+    assert 0 < r["mine"].size < len(suns)
+    one = OracleBatch([(files.scene, files.config)], [(0, s) for s in suns], tmp_path)
+    one.trace()
+    for k in range(len(suns)):
+        assert np.array_equal(r[f"image{k}"], one.image(k, 0))
+        assert np.array_equal(r[f"per{k}"], one.power(k)[0])
+
+
+def test_sun_split_adjoint_reduces_to_one_pair(tmp_path):
+    """The pair over 5 suns split over two gloo ranks by ShardedDiff (a linear
+    stand-in pair on the host): the all-reduced loss and gradient equal one
+    pair over all 5 suns to FP64 summation order."""
+    from tests.shard_models import LinearPair
+
+    r = _run_ranks(None, None, tmp_path / "d.npz", argv=["diff", str(tmp_path / "d.npz")])
+    H = 7
+    suns = np.array([[0.1 * k, -1.0, 0.05 * k] for k in range(5)], np.float32)  # as ShardedDiff holds them
+    one = LinearPair(suns, H)
+    rng = np.random.default_rng(3)
+    for k in range(5):
+        one.set_target(rng.standard_normal(40), receiver=k)
+    one.set_params(rng.standard_normal((H, 2)), rng.standard_normal((H, 2)))
+    assert (int(r["begin"]), int(r["end"])) == (0, 3)
+    assert float(r["loss"]) == pytest.approx(one.forward(), rel=1e-12)
+    np.testing.assert_allclose(r["grad"], one.backward(), rtol=1e-12, atol=1e-12)
