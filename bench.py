@@ -231,7 +231,7 @@ def batched_vs_plain(torch, scene, lights: int, stream, num_fields: int = 16, se
     inst = [(0, sun) for sun in suns] + [(1 + k, sun) for k, (_, sun) in enumerate(work[len(suns):])]
     batch = q.Batch(scenes, inst)
     batch.set_light_range(0, lights)
-    mode, _ = batch.autotune(stream)
+    shape, shape_ms = batch.autotune(stream)
     batch.capture_graph(clear_first=True)
     batch.graph_launch(stream)  # warm-up
     torch.cuda.synchronize()
@@ -255,7 +255,7 @@ def batched_vs_plain(torch, scene, lights: int, stream, num_fields: int = 16, se
     scene.set_sun(own_sun)
     return {"suns": len(suns), "fields": num_fields,
             "field_heliostats": [f.num_heliostats for f in fields], "lights_per_instance": lights, "rays": rays,
-            "autotuned_mode": mode,
+            "autotuned_shape": {"chosen": shape, "shapes": q.launch_shapes(), "ms_per_shape": shape_ms},
             "plain_looped_mrays_s": rays / (plain_ms / 1e3) / 1e6, "batched_mrays_s": rays / (batched_ms / 1e3) / 1e6,
             "batched_graph_only_mrays_s": rays / (kernel_ms / 1e3) / 1e6,
             "speedup_batched_vs_plain": plain_ms / batched_ms, "plain_ms": plain_ms, "batched_ms": batched_ms}

@@ -146,6 +146,19 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* scene, unsigned seed);
  * and energy: hits near a pixel boundary or the cylinder's silhouette can
  * land one pixel over or flip, as in the reference's own CUDA build). */
 int qmcrt_set_math_mode(qmcrt_scene* scene, int exact);
+/* Launch shapes of the production build (math mode 0), indexes 0..count-1:
+ * threads per block and warp-chunk iterations (32 rays each); shape 0 is the
+ * default.  No reference counterpart: the reference launches 512-thread
+ * blocks of one ray each (Util/global_function.cuh:159-197).  Any array may
+ * be NULL; at most 16 shapes. */
+int qmcrt_launch_shapes(int* threads, int* chunk_iters, int* count);
+int qmcrt_set_launch_shape(qmcrt_scene* scene, int shape);
+/* Autotuner: traces heliostats[0..n) over the current light range once per
+ * launch shape of the production build (after one warm-up each), keeps the
+ * fastest for the scene's flux launches and reports it (best) and every
+ * shape's device time in ms (ms_per_shape, may be NULL).  Images and powers
+ * are cleared after.  The scene must be in math mode 0. */
+int qmcrt_autotune(qmcrt_scene* scene, const int* heliostats, int n, void* stream, int* best, float* ms_per_shape);
 /* Trace only light indexes [begin, end) of every facet (default [0, per_group)).
  * Energies keep the full-trace factor DNI*(hpx/rpx)^2*rho/per_group. */
 int qmcrt_set_light_range(qmcrt_scene* scene, int begin, int end);
@@ -253,9 +266,15 @@ int qmcrt_batch_graph_launch(qmcrt_batch* batch, void* stream);
 int qmcrt_batch_clear(qmcrt_batch* batch, void* stream);
 int qmcrt_batch_image(qmcrt_batch* batch, int instance, int receiver, float* out, int* width, int* height);
 int qmcrt_batch_power_fp64(qmcrt_batch* batch, int instance, double* per_heliostat, double* total);
-/* Times the production kernel builds (modes 0 and 2, identical results) on
- * this batch and keeps the faster; images and powers are cleared after. */
-int qmcrt_batch_autotune(qmcrt_batch* batch, void* stream, int* chosen_mode, float* ms);
+/* Autotuner over the production build's launch shapes (qmcrt_launch_shapes;
+ * identical per-ray arithmetic, so identical results up to the order of
+ * float additions): times each on this batch, keeps the fastest in math mode
+ * 0 and reports its index; ms_per_shape (may be NULL) receives every
+ * shape's time.  Images and powers are cleared after.  qmcrt_batch_autotune
+ * is the same with only the chosen shape's time. */
+int qmcrt_batch_autotune_shapes(qmcrt_batch* batch, void* stream, int* chosen_shape, float* ms_per_shape);
+int qmcrt_batch_autotune(qmcrt_batch* batch, void* stream, int* chosen_shape, float* ms);
+int qmcrt_batch_set_launch_shape(qmcrt_batch* batch, int shape);
 /* Debug: the device-prepared sub-heliostat vertices (B, A, C per
  * sub-heliostat, as qmcrt_grid_vertices) of one instance-grid and the
  * heliostat normals of one instance (either output may be NULL). */

@@ -16,6 +16,7 @@ from .scene import (  # noqa: F401
     RayTracingPipeline,
     Scene,
     executable,
+    launch_shapes,
     pipeline_run,
     save_text,
     smooth_device,
@@ -24,5 +25,5 @@ from .scene import (  # noqa: F401
 __all__ = [
     "Scene", "Batch", "Diff", "QuasiMonteCarloRayTracer", "ImageSmoother", "ImageSaver", "RayTracingPipeline",
     "SUNSHAPE_BUIE", "SUNSHAPE_PILLBOX", "QmcrtError", "load", "LIB_PATH", "save_text", "smooth_device",
-    "pipeline_run", "executable",
+    "pipeline_run", "executable", "launch_shapes",
 ]

@@ -94,6 +94,11 @@ PROTOTYPES = {
     "qmcrt_batch_image": (_i, [_vp, _i, _i, _pf, _pi, _pi]),
     "qmcrt_batch_power_fp64": (_i, [_vp, _i, _pd, _pd]),
     "qmcrt_batch_autotune": (_i, [_vp, _vp, _pi, _pf]),
+    "qmcrt_batch_autotune_shapes": (_i, [_vp, _vp, _pi, _pf]),
+    "qmcrt_batch_set_launch_shape": (_i, [_vp, _i]),
+    "qmcrt_launch_shapes": (_i, [_pi, _pi, _pi]),
+    "qmcrt_set_launch_shape": (_i, [_vp, _i]),
+    "qmcrt_autotune": (_i, [_vp, _pi, _i, _vp, _pi, _pf]),
     "qmcrt_batch_debug_geometry": (_i, [_vp, _i, _i, _pf, _pf]),
     "qmcrt_diff_create": (_i, [_vp, _f, ctypes.POINTER(_vp)]),
     "qmcrt_diff_free": (None, [_vp]),

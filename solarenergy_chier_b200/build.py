@@ -42,9 +42,19 @@ CUDA_UNITS = [
                                         "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
                                         "-fmad=false"]),
+    # launch shapes of the production build timed by the autotuner (qmcrt_autotune):
+    # warp chunks of 32 or 128 iterations, two-warp blocks
+    ("tracer.cu", "tracer_fast_c32.o", ["-DQM_TRACE_VARIANT=fast_c32", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
+                                           "-DQM_CHUNK_ITERS=32", "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS"]),
+    ("tracer.cu", "tracer_fast_c128.o", ["-DQM_TRACE_VARIANT=fast_c128", "-DQM_TRACE_THREADS=32",
+                                            "-DQM_TRACE_MIN_BLOCKS=28", "-DQM_CHUNK_ITERS=128", "-DQM_TRACE_FAST_DIVIDE",
+                                            "-DQM_TRACE_CANDIDATE_HITS"]),
+    ("tracer.cu", "tracer_fast_t64.o", ["-DQM_TRACE_VARIANT=fast_t64", "-DQM_TRACE_THREADS=64", "-DQM_TRACE_MIN_BLOCKS=14",
+                                           "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_approx.o", ["-DQM_TRACE_VARIANT=approx", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
                                          "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS", "-DQM_TRACE_APPROX_MATH"]),
     ("pools.cu", "pools.o", []),
+    ("power.cu", "power.o", []),
     # per-sun preparation: no FMA contraction, so it matches the host geometry bit for bit
     ("prep.cu", "prep.o", ["-fmad=false"]),
     ("diff.cu", "diff_kernels.o", []),

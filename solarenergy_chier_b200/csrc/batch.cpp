@@ -106,7 +106,7 @@ void batch_prepare(qmcrt_batch* b, cudaStream_t st) {
 
 void batch_build_prefix(qmcrt_batch* b) {
   const long long nl = b->light_end - b->light_begin;
-  const long long chunk = trace_chunk_rays();
+  const long long chunk = chunk_rays_for(b->mode, b->shape, 0);
   std::vector<long long> prefix(b->tasks.size() + 1, 0);
   for (size_t i = 0; i < b->tasks.size(); ++i) {
     const long long rays = (long long)b->tasks[i].num_facets * nl;
@@ -115,6 +115,8 @@ void batch_build_prefix(qmcrt_batch* b) {
   }
   upload(b->d_prefix, prefix);
   b->total_chunks = prefix.back();
+  // allocated here, before any graph capture of the launch
+  chunk_power_buffer(b->d_chunk_power, b->total_chunks);
 }
 
 cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chunk_begin, long long chunk_end) {
@@ -131,7 +133,10 @@ cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chu
   p.power = b->d_power.as<double>();
   p.diag = b->d_diag.as<unsigned long long>();
   p.hit_bits = b->hit_bits;
-  return launch_trace_mode(b->mode, p, out, st);
+  if (out == 0 || out == 2) p.chunk_power = b->d_chunk_power.as<double>();
+  // the prefix is laid out for the flux kernel's chunk size
+  if (chunk_rays_for(b->mode, b->shape, out) != chunk_rays_for(b->mode, b->shape, 0)) return cudaErrorInvalidValue;
+  return launch_trace_mode(b->mode, p, out, st, b->shape);
 }
 
 }  // namespace qrt
@@ -447,23 +452,27 @@ int qmcrt_batch_debug_geometry(qmcrt_batch* b, int k, int grid, float* vertices,
   });
 }
 
-int qmcrt_batch_autotune(qmcrt_batch* b, void* stream, int* chosen, float* ms) {
+int qmcrt_batch_autotune_shapes(qmcrt_batch* b, void* stream, int* chosen, float* ms_per_shape) {
   return guarded([&] {
     batch_checked(b);
     DeviceGuard guard(b->device);
-    if (b->total_chunks < 0) batch_build_prefix(b);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // Candidates give identical results (same arithmetic, different register
-    // budgets and occupancy); time each on the batch itself and keep the
-    // fastest.  Images and powers are cleared afterwards.
-    const int candidates[2] = {0, 2};
+    // The candidates are the production build's launch shapes: identical
+    // per-ray arithmetic, different block widths, register budgets and warp
+    // chunks.  Each is timed on the batch itself (its prefix rebuilt for the
+    // shape's chunk size) and the fastest kept.  Images and powers are
+    // cleared afterwards.
+    int n_shapes = 0;
+    qmcrt_launch_shapes(nullptr, nullptr, &n_shapes);
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
     cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
     float best = 1e30f;
     int pick = 0;
-    for (int c : candidates) {
-      b->mode = c;
+    b->mode = 0;
+    for (int k = 0; k < n_shapes; ++k) {
+      b->shape = k;
+      batch_build_prefix(b);
       cuda_check(batch_launch(b, st, 0), "autotune");  // warm-up
       cudaEventRecord(e0, st);
       cuda_check(batch_launch(b, st, 0), "autotune");
@@ -471,19 +480,43 @@ int qmcrt_batch_autotune(qmcrt_batch* b, void* stream, int* chosen, float* ms) {
       cuda_check(cudaEventSynchronize(e1), "autotune");
       float t = 0.f;
       cudaEventElapsedTime(&t, e0, e1);
+      if (ms_per_shape) ms_per_shape[k] = t;
       if (t < best) {
         best = t;
-        pick = c;
+        pick = k;
       }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    b->mode = pick;
+    b->shape = pick;
+    batch_build_prefix(b);
     b->drop_graph();
     clear_async(b, st);
     cuda_check(cudaStreamSynchronize(st), "autotune");
     if (chosen) *chosen = pick;
-    if (ms) *ms = best;
+  });
+}
+
+int qmcrt_batch_autotune(qmcrt_batch* b, void* stream, int* chosen, float* ms) {
+  float table[16] = {0};
+  int pick = 0;
+  const int rc = qmcrt_batch_autotune_shapes(b, stream, &pick, table);
+  if (rc == QMCRT_OK) {
+    if (chosen) *chosen = pick;
+    if (ms) *ms = table[pick];
+  }
+  return rc;
+}
+
+int qmcrt_batch_set_launch_shape(qmcrt_batch* b, int shape) {
+  return guarded([&] {
+    batch_checked(b);
+    int n_shapes = 0;
+    qmcrt_launch_shapes(nullptr, nullptr, &n_shapes);
+    if (shape < 0 || shape >= n_shapes) invalid("launch shape out of range");
+    b->shape = shape;
+    b->total_chunks = -1;
+    b->drop_graph();
   });
 }
 

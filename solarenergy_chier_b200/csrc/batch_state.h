@@ -26,9 +26,11 @@ struct qmcrt_batch {
   qrt::DBuf d_grids, d_receivers, d_tasks, d_prefix, d_items, d_rot;
   qrt::DBuf d_bound, d_hsub, d_subv, d_verts, d_sub_free, d_sub_cand, d_sub_frames;  // per instance-grid slices
   qrt::DBuf d_images, d_power, d_diag, d_pools;
+  qrt::DBuf d_chunk_power;  // per-chunk FP64 power partials of a launch (sized with the chunk prefix)
   int light_begin = 0, light_end = 0, max_lights = 0;
   long long total_chunks = -1;  // for the current light range; -1 = prefix not built
-  int mode = 0;                 // 0 production, 1 exact, 2 production at 64 registers
+  int mode = 0;                 // 0 production, 1 exact, 2 production at 64 registers, 3 approximate math
+  int shape = 0;                // launch shape of the production build (qmcrt_batch_set_launch_shape)
   uint32_t* hit_bits = nullptr;  // output of bilinear-deposit launches (owned by the caller)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -46,7 +48,8 @@ struct qmcrt_batch {
     cudaDeviceSynchronize();
     drop_graph();
     for (qrt::DBuf* b : {&d_grids, &d_receivers, &d_tasks, &d_prefix, &d_items, &d_rot, &d_bound, &d_hsub, &d_subv,
-                    &d_verts, &d_sub_free, &d_sub_cand, &d_sub_frames, &d_images, &d_power, &d_diag, &d_pools})
+                    &d_verts, &d_sub_free, &d_sub_cand, &d_sub_frames, &d_images, &d_power, &d_diag, &d_pools,
+                    &d_chunk_power})
       b->release();
     cudaSetDevice(prev);
   }

@@ -3,6 +3,7 @@
 #include "helio_geom.h"
 #include "prep.h"
 #include "grid_build.h"
+#include "power.h"
 
 #include <cuda_runtime.h>
 
@@ -429,17 +430,53 @@ qm::TraceParams base_params(qmcrt_scene* s) {
   return p;
 }
 
-cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st) {
+// Launch shapes of the production build (math mode 0) that the autotuner
+// times: threads per block and warp-chunk iterations, all at 72 registers
+// except the 256-thread shape (64 registers, as math mode 2).  A shape
+// changes how rays are handed to warps, never a ray's arithmetic.  Shapes
+// other than 0 serve flux launches only; records, hit bits and bilinear
+// deposits keep shape 0, whose chunk layout the other outputs share.
+struct LaunchShape {
+  int threads, chunk_iters;
+  cudaError_t (*launch)(const qm::TraceParams&, int, cudaStream_t);
+  int (*chunk_rays)();
+};
+const LaunchShape kShapes[] = {
+    {32, 64, qm::launch_trace_fast, qm::trace_chunk_rays_fast},
+    {32, 32, qm::launch_trace_fast_c32, qm::trace_chunk_rays_fast_c32},
+    {32, 128, qm::launch_trace_fast_c128, qm::trace_chunk_rays_fast_c128},
+    {64, 64, qm::launch_trace_fast_t64, qm::trace_chunk_rays_fast_t64},
+    {256, 64, qm::launch_trace_fast4, qm::trace_chunk_rays_fast4},
+};
+constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
+
+int shape_for(int mode, int shape, int out) { return (mode == 0 && out == 0 && shape > 0 && shape < kNumShapes) ? shape : 0; }
+
+long long chunk_rays_for(int mode, int shape, int out) {
+  return kShapes[shape_for(mode, shape, out)].chunk_rays();
+}
+
+cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st, int shape) {
+  cudaError_t e;
   switch (mode) {
-    case 1: return qm::launch_trace_exact(p, out, st);
-    case 2: return qm::launch_trace_fast4(p, out, st);
-    case 3: return qm::launch_trace_approx(p, out, st);
-    default: return qm::launch_trace_fast(p, out, st);
+    case 1: e = qm::launch_trace_exact(p, out, st); break;
+    case 2: e = qm::launch_trace_fast4(p, out, st); break;
+    case 3: e = qm::launch_trace_approx(p, out, st); break;
+    default: e = kShapes[shape_for(mode, shape, out)].launch(p, out, st); break;
   }
+  // flux and bilinear-deposit launches add their per-chunk power partials
+  if (e == cudaSuccess && (out == 0 || out == 2) && p.chunk_power) e = qm::launch_power_reduce(p, st);
+  return e;
+}
+
+double* chunk_power_buffer(DBuf& buf, long long chunks) {
+  const size_t need = (size_t)std::max<long long>(chunks, 1) * sizeof(double);
+  if (buf.bytes < need) buf.alloc(need);
+  return buf.as<double>();
 }
 
 cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st) {
-  return launch_trace_mode(s->exact, p, out, st);
+  return launch_trace_mode(s->exact, p, out, st, s->shape);
 }
 
 // Traces heliostats ids[0..n) over the scene's light range: out 0 adds their
@@ -457,9 +494,9 @@ long long trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream, 
   DeviceGuard guard(s->device);
   const long long nl = s->light_end - s->light_begin;
   if (nl == 0) return 0;
-  const long long chunk = qm::trace_chunk_rays_fast();
+  const long long chunk = chunk_rays_for(s->exact, s->shape, out);
   auto chunks_of = [&](int id) { return ((long long)s->templates[id].num_facets * nl + chunk - 1) / chunk; };
-  bool same = s->cache_valid && s->cached_lights == nl && (int)s->cached_ids.size() == n &&
+  bool same = s->cache_valid && s->cached_lights == nl && s->cached_chunk == chunk && (int)s->cached_ids.size() == n &&
               std::equal(ids, ids + n, s->cached_ids.begin());
   long long total = 0;
   if (!same) {
@@ -477,6 +514,7 @@ long long trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream, 
     cuda_check(cudaEventRecord(s->stage_done, stream), "cudaEventRecord");
     s->cached_ids.assign(ids, ids + n);
     s->cached_lights = nl;
+    s->cached_chunk = chunk;
     s->cache_valid = true;
   }
   for (int i = 0; i < n; ++i) total += chunks_of(ids[i]);
@@ -487,6 +525,7 @@ long long trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream, 
   p.total_facets = total;
   p.hit_bits = hit_bits;
   if (out == 3 && !hit_bits) return total;
+  if (out == 0) p.chunk_power = chunk_power_buffer(s->d_chunk_power, total);
   cuda_check(run_trace(s, p, out, stream), "trace kernel");
   return total;
 }
@@ -833,6 +872,60 @@ int qmcrt_trace_heliostat(qmcrt_scene* s, int id, void* stream) {
 
 int qmcrt_trace_heliostats(qmcrt_scene* s, const int* ids, int n, void* stream) {
   return guarded([&] { trace_ids(checked(s), ids, n, static_cast<cudaStream_t>(stream)); });
+}
+
+int qmcrt_launch_shapes(int* threads, int* chunk_iters, int* count) {
+  return guarded([&] {
+    if (count) *count = kNumShapes;
+    for (int k = 0; k < kNumShapes; ++k) {
+      if (threads) threads[k] = kShapes[k].threads;
+      if (chunk_iters) chunk_iters[k] = kShapes[k].chunk_iters;
+    }
+  });
+}
+
+int qmcrt_set_launch_shape(qmcrt_scene* s, int shape) {
+  return guarded([&] {
+    checked(s);
+    if (shape < 0 || shape >= kNumShapes) invalid("launch shape out of range");
+    s->shape = shape;
+  });
+}
+
+int qmcrt_autotune(qmcrt_scene* s, const int* ids, int n, void* stream, int* best, float* ms_per_shape) {
+  return guarded([&] {
+    checked(s);
+    if (s->exact != 0) throw ApiError(QMCRT_ERR_STATE, "the launch shapes belong to the production build (math mode 0)");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DeviceGuard guard(s->device);
+    cudaEvent_t e0, e1;
+    cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
+    cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
+    float best_ms = 1e30f;
+    int pick = 0;
+    for (int k = 0; k < kNumShapes; ++k) {
+      s->shape = k;
+      trace_ids(s, ids, n, st);  // warm-up (and the task upload for this chunk size)
+      cuda_check(cudaEventRecord(e0, st), "cudaEventRecord");
+      trace_ids(s, ids, n, st);
+      cuda_check(cudaEventRecord(e1, st), "cudaEventRecord");
+      cuda_check(cudaEventSynchronize(e1), "autotune");
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (ms_per_shape) ms_per_shape[k] = t;
+      if (t < best_ms) {
+        best_ms = t;
+        pick = k;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->shape = pick;
+    for (auto& img : s->images) cuda_check(cudaMemsetAsync(img->p, 0, img->bytes, st), "image clear");
+    cuda_check(cudaStreamSynchronize(st), "autotune");
+    cuda_check(cudaMemset(s->d_power.p, 0, s->d_power.bytes), "clear");
+    if (best) *best = pick;
+  });
 }
 
 int qmcrt_debug_hit_bits(qmcrt_scene* s, const int* ids, int n, unsigned* device_bits, long long capacity,

@@ -113,6 +113,11 @@ struct TraceParams {
   int light_begin, light_end;     // light indexes traced per facet
   int lights_q32, lights_r32;     // 32 / (light_end - light_begin) and 32 % it (set by the launcher)
   double* power;                  // FP64 per-slot power accumulators
+  // flux and bilinear-deposit launches: when set, each warp chunk writes its
+  // rays' FP64 energy sum to chunk_power[chunk - chunk_begin] and
+  // launch_power_reduce (power.cu) adds them per task into power, in a fixed
+  // order with compensation; when NULL, one double atomic per chunk
+  double* chunk_power;
   unsigned long long* diag;
   // bilinear-deposit and hit-bit variants: one word per warp iteration of the
   // launch (chunk - chunk_begin), bit i = lane i's ray hit the receiver; may

@@ -144,10 +144,13 @@ struct qmcrt_scene {
   qrt::DBuf d_offset_seg;     // heliostats + 1 starts of the per-heliostat offset segments
   int pool_size = 0;
   qrt::DBuf d_power, d_diag;
+  qrt::DBuf d_chunk_power;  // per-chunk FP64 power partials of a launch (grows to the largest launch)
   std::vector<qm::DevTask> templates;
   qrt::DBuf d_tasks, d_prefix;
   std::vector<int> cached_ids;
   long long cached_lights = -1;
+  long long cached_chunk = -1;
+  int shape = 0;  // launch shape of the production build (qmcrt_set_launch_shape)
   bool cache_valid = false;
   qm::DevTask* h_stage = nullptr;  // pinned staging for task uploads
   long long* h_prefix = nullptr;
@@ -183,6 +186,7 @@ struct qmcrt_scene {
     d_trace_perturb.release();
     d_offset_seg.release();
     d_power.release();
+    d_chunk_power.release();
     d_diag.release();
     d_tasks.release();
     d_prefix.release();
@@ -202,7 +206,11 @@ qmcrt_scene* checked(qmcrt_scene* s);
 void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world);
 // out: 0 flux, 1 per-ray outcome codes, 2 bilinear deposit, 3 hit bits
 // (qm::TraceOut in tracer.cu); mode: the kernel build (qmcrt_set_math_mode).
-cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st);
+cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st, int shape = 0);
+// Rays per warp chunk of the kernel a launch of (mode, shape, out) runs.
+long long chunk_rays_for(int mode, int shape, int out);
+// Grow-only buffer of per-chunk power partials for a launch of `chunks` warp chunks.
+double* chunk_power_buffer(DBuf& buf, long long chunks);
 cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st);
 int trace_chunk_rays();
 constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;

@@ -623,7 +623,8 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   }
   flags = __reduce_or_sync(0xffffffffu, flags);
   if (lane == 0) {
-    if (power != 0.0) atomicAdd(p.power + T.power_slot, power);
+    if (p.chunk_power && kOut != kOutRecord) p.chunk_power[warp] = power;
+    else if (power != 0.0) atomicAdd(p.power + T.power_slot, power);
     if (clamped) atomicAdd(p.diag + kDiagClamped, clamped);
     if (flags & 2u) atomicAdd(p.diag + kDiagDdaCap, 1ull);
   }

@@ -16,6 +16,14 @@ cudaError_t launch_trace_fast(const TraceParams& p, int out, cudaStream_t stream
 cudaError_t launch_trace_exact(const TraceParams& p, int out, cudaStream_t stream);
 // Production build limited to 64 registers (four 256-thread blocks per SM).
 cudaError_t launch_trace_fast4(const TraceParams& p, int out, cudaStream_t stream);
+// Production build in other launch shapes (the autotuner's candidates):
+// 32-iteration and 128-iteration warp chunks, two-warp blocks.
+cudaError_t launch_trace_fast_c32(const TraceParams& p, int out, cudaStream_t stream);
+cudaError_t launch_trace_fast_c128(const TraceParams& p, int out, cudaStream_t stream);
+cudaError_t launch_trace_fast_t64(const TraceParams& p, int out, cudaStream_t stream);
+int trace_chunk_rays_fast_c32();
+int trace_chunk_rays_fast_c128();
+int trace_chunk_rays_fast_t64();
 // Production build with approximate per-ray arithmetic after the shadow test
 // (FMA contraction, hardware reciprocal square root, approximate divisions).
 cudaError_t launch_trace_approx(const TraceParams& p, int out, cudaStream_t stream);

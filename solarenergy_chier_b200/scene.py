@@ -177,6 +177,20 @@ class Scene:
     def set_light_range(self, begin: int, end: int) -> None:
         check(self._lib.qmcrt_set_light_range(self._h, begin, end))
 
+    def set_launch_shape(self, shape: int) -> None:
+        """Launch shape of the production build's flux launches (launch_shapes())."""
+        check(self._lib.qmcrt_set_launch_shape(self._h, int(shape)))
+
+    def autotune(self, heliostats, stream=None) -> tuple[int, list]:
+        """Times every launch shape on `heliostats` at the current light range and
+        keeps the fastest: (chosen shape, ms per shape).  Clears images and powers."""
+        ids = np.ascontiguousarray(np.atleast_1d(np.asarray(heliostats, np.int32)))
+        best = ctypes.c_int()
+        table = (ctypes.c_float * 16)()
+        check(self._lib.qmcrt_autotune(self._h, _ptr(ids, ctypes.c_int), ids.size, _stream_handle(stream),
+                                       ctypes.byref(best), table))
+        return best.value, list(table[: len(launch_shapes())])
+
     def shadow_free(self) -> np.ndarray:
         """Per heliostat: 1 shadow walks skipped, k + 1 only k listed candidate
         shadowing heliostats (rays missing their boxes skip the walk), 0 walk."""
@@ -352,10 +366,16 @@ class Batch:
     def clear(self, stream=None) -> None:
         check(self._lib.qmcrt_batch_clear(self._h, _stream_handle(stream)))
 
-    def autotune(self, stream=None) -> tuple[int, float]:
-        m, ms = ctypes.c_int(), ctypes.c_float()
-        check(self._lib.qmcrt_batch_autotune(self._h, _stream_handle(stream), ctypes.byref(m), ctypes.byref(ms)))
-        return m.value, ms.value
+    def autotune(self, stream=None) -> tuple[int, list]:
+        """Times every launch shape of the production build on this batch and
+        keeps the fastest: (chosen shape, ms per shape)."""
+        m = ctypes.c_int()
+        table = (ctypes.c_float * 16)()
+        check(self._lib.qmcrt_batch_autotune_shapes(self._h, _stream_handle(stream), ctypes.byref(m), table))
+        return m.value, list(table[: len(launch_shapes())])
+
+    def set_launch_shape(self, shape: int) -> None:
+        check(self._lib.qmcrt_batch_set_launch_shape(self._h, int(shape)))
 
     def image(self, instance: int, receiver: int = 0) -> np.ndarray:
         w, h = ctypes.c_int(), ctypes.c_int()
@@ -538,6 +558,17 @@ class RayTracingPipeline:
     @staticmethod
     def rayTracing(argv: list[str]) -> int:  # noqa: N802
         return pipeline_run(argv)
+
+
+def launch_shapes() -> list[tuple[int, int]]:
+    """(threads per block, warp-chunk iterations) of each launch shape of the production build."""
+    lib = load()
+    n = ctypes.c_int()
+    check(lib.qmcrt_launch_shapes(None, None, ctypes.byref(n)))
+    t = np.zeros(n.value, np.int32)
+    c = np.zeros(n.value, np.int32)
+    check(lib.qmcrt_launch_shapes(_ptr(t, ctypes.c_int), _ptr(c, ctypes.c_int), ctypes.byref(n)))
+    return list(zip(t.tolist(), c.tolist()))
 
 
 def executable() -> Path:

@@ -95,8 +95,9 @@ def test_graph_replay_and_set_suns(fields):
 def test_autotune_and_errors(fields):
     scenes = scenes_of(fields)
     b = q.Batch(scenes, [(0, SUNS[0]), (1, SUNS[1])])
-    mode, ms = b.autotune()
-    assert mode in (0, 2) and ms > 0
+    shape, ms = b.autotune()
+    assert 0 <= shape < len(q.launch_shapes()) and len(ms) == len(q.launch_shapes()) and min(ms) > 0
+    assert ms[shape] == min(ms)
     assert b.power(0)[1] == 0.0  # autotune clears
     with pytest.raises(q.QmcrtError):
         b.set_light_range(0, 10 ** 6)
@@ -129,3 +130,52 @@ def test_uneven_fields_batch_equals_plain(tmp_path):
         gper, gtotal = b.power(k)
         assert abs(gtotal - total) <= 1e-9 * total
         assert np.allclose(gper, per, rtol=1e-9, atol=0)
+
+
+def test_every_launch_shape_gives_the_same_result(fields, tmp_path):
+    """The autotuner's candidates (launch shapes of the production build:
+    block widths, warp chunks of 32, 64 or 128 iterations) change only how
+    rays are handed to warps: every shape gives the same flux (up to float
+    atomic order, L1 <= 1e-6) and FP64 powers (1e-12) on a plain scene and
+    on a batch, with ragged light counts (37 lights: warps span facets and
+    chunks end inside one), and the plain autotuner keeps the fastest."""
+    shapes = q.launch_shapes()
+    assert shapes[0] == (32, 64) and len(shapes) >= 4
+    f = fields[1]
+    s = q.Scene(f.scene, f.config, device=0, seed=4)
+    ids = list(range(s.num_heliostats))
+    s.set_light_range(3, 40)
+    ref = None
+    for k in range(len(shapes)):
+        s.set_launch_shape(k)
+        s.clear()
+        s.clear_power()
+        s.trace(ids)
+        img = s.image(0).astype(np.float64)
+        per, total = s.power()
+        if ref is None:
+            ref = (img, per, total)
+            assert total > 0
+            continue
+        assert np.abs(img - ref[0]).sum() <= 1e-6 * ref[0].sum(), shapes[k]
+        np.testing.assert_allclose(per, ref[1], rtol=1e-12, atol=0)
+    best, ms = s.autotune(ids)
+    assert ms[best] == min(ms) and min(ms) > 0
+    assert s.power()[1] == 0.0
+    s.trace(ids)  # the chosen shape traces like the others
+    assert abs(s.power()[1] - ref[2]) <= 1e-12 * ref[2]
+    scenes = scenes_of(fields)
+    b = q.Batch(scenes, [(0, SUNS[0]), (1, SUNS[1])])
+    b.set_light_range(1, 38)
+    first = None
+    for k in range(len(shapes)):
+        b.set_launch_shape(k)
+        b.clear()
+        b.trace()
+        out = [(b.image(i).astype(np.float64), b.power(i)[1]) for i in range(2)]
+        if first is None:
+            first = out
+            continue
+        for (img, tot), (img0, tot0) in zip(out, first):
+            assert np.abs(img - img0).sum() <= 1e-6 * img0.sum()
+            assert abs(tot - tot0) <= 1e-12 * tot0
