@@ -317,3 +317,67 @@ def test_adjoint_on_a_slice_of_the_benchmark_field(tmp_path, cuda_device):
     d.close()
     s.close()
     assert not failures, failures
+
+
+def test_large_field_errors_against_fp64_on_a_subsample(tmp_path, cuda_device):
+    """The large batched-adjoint configuration's rays against FP64 on a 1 %
+    subsample: the 10,000-heliostat field (flat 10 x 10 m heliostats, 0.05 m
+    micro-facets: 40,000 each, 150-1800 m, cylinder r 10 m x h 20 m at 200 m),
+    every 100th heliostat x its 40,000 facets x light indexes 0-3 (1.6e7
+    rays), at 2 of the 32 suns the large adjoint traces.  The plain tracer's
+    rays are the forward's rays (the same hits: tests above), so their
+    errors are the forward's.  Reported per sun: flux L1, per-heliostat and
+    total power against the FP64 oracle, beside the reference's float
+    arithmetic (the CPU oracle in float) on the same rays.  Bars (written
+    here): the tracer within 1e-3 flux L1 and 1e-5 total power of the
+    reference's float arithmetic, and no further from FP64 than it
+    (1.05 x + 1e-4 in L1, + 2e-6 in power)."""
+    import json
+
+    from oracle import oracle
+
+    files = synth.huge_field(tmp_path, seed=0)
+    s = q.Scene(files.scene, files.config, device=0, seed=3)
+    H = s.num_heliostats
+    assert H == 10000 and s.heliostat(0)["num_facets"] == 40000
+    ids = list(range(0, H, 100))
+    dirs, pert = s.get_sample_pool()
+    offsets = {h: s.get_facet_offsets(h) for h in ids}
+    suns = synth.sun_positions()[::3][:32]
+    lights = 4
+    s.set_light_range(0, lights)
+    for k in (0, 17):
+        sun = suns[k]
+        s.set_sun(sun)
+        s.clear()
+        s.clear_power()
+        s.trace(ids)
+        img = s.image(0).astype(np.float64)
+        per, total = s.power()
+        cfg = json.loads(files.config.read_text())
+        cfg["sun_dir"] = [float(x) for x in sun]
+        cpath = tmp_path / f"sun{k}.json"
+        cpath.write_text(json.dumps(cfg))
+        r32 = oracle.OracleScene.from_files(files.scene, cpath).trace(ids, dirs, pert, offsets, 0, lights)
+        r64 = oracle.OracleScene.from_files(files.scene, cpath, precision=64).trace(ids, dirs, pert, offsets, 0,
+                                                                                   lights)
+        i32, i64 = r32["images"][0], r64["images"][0]
+        t32, t64 = float(r32["power"].sum()), float(r64["power"].sum())
+        assert t64 > 0
+
+        def l1(a, b):
+            return float(np.abs(a - b).sum() / b.sum())
+
+        sel = np.array(ids)
+        rep = {"sun": k, "rays": r32["counters"]["rays"], "flux_l1_vs_fp64": l1(img, i64),
+               "reference_arithmetic_flux_l1_vs_fp64": l1(i32, i64), "flux_l1_vs_reference_arithmetic": l1(img, i32),
+               "power_rel_vs_fp64": abs(total - t64) / t64,
+               "reference_arithmetic_power_rel_vs_fp64": abs(t32 - t64) / t64,
+               "max_heliostat_power_rel_vs_fp64": float(np.max(np.abs(per[sel] - r64["power"][sel]) /
+                                                               np.maximum(r64["power"][sel], 1e-30)))}
+        print("large field, 1 % subsample:", json.dumps(rep))
+        assert rep["flux_l1_vs_reference_arithmetic"] <= 1e-3
+        assert abs(total - t32) <= 1e-5 * t32
+        assert rep["flux_l1_vs_fp64"] <= 1.05 * rep["reference_arithmetic_flux_l1_vs_fp64"] + 1e-4
+        assert rep["power_rel_vs_fp64"] <= rep["reference_arithmetic_power_rel_vs_fp64"] + 2e-6
+    s.close()
