@@ -41,7 +41,7 @@ CUDA_UNITS = [
     ("tracer.cu", "tracer_fast4.o", ["-DQM_TRACE_VARIANT=fast4", "-DQM_TRACE_MIN_BLOCKS=4", "-DQM_TRACE_FAST_DIVIDE",
                                         "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_exact.o", ["-DQM_TRACE_VARIANT=exact", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
-                                        "-fmad=false"]),
+                                        "-DQM_EXACT_ACOS", "-fmad=false"]),
     # launch shapes of the production build timed by the autotuner (qmcrt_autotune):
     # warp chunks of 32 or 128 iterations, two-warp blocks
     ("tracer.cu", "tracer_fast_c32.o", ["-DQM_TRACE_VARIANT=fast_c32", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",

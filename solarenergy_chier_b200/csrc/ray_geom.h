@@ -42,6 +42,15 @@ __device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, flo
   // the quotient is within a double ulp of a float rounding boundary
   // (about 2^-29 of rays).
   v = (float)((double)acosf(cx) * (1.0 / (2 * M_PI)));
+#elif defined(QM_EXACT_ACOS)
+  // The exact build evaluates the arc cosine in double and rounds it once
+  // to float: the correctly rounded value, which the host C library's float
+  // acosf (what the reference's host build and the CPU oracle call; glibc
+  // 2.39 on this image) returns for all but 0.25 % of the floats in
+  // [-1, 1].  The device's own acosf differs from the host's far more often
+  // (about 4 hits in a million landed one column over at the benchmark
+  // field); through the double evaluation about 6 in 10^8 do.
+  v = (float)__ddiv_rn((double)(float)acos((double)cx), 2 * M_PI);
 #else
   v = (float)__ddiv_rn((double)acosf(cx), 2 * M_PI);
 #endif
@@ -70,8 +79,8 @@ __device__ __forceinline__ bool cylinder_hit_approx(const DevReceiver& r, float3
   const float tp = -(lx * d.x + lz * d.z) * il;
   const float delta = (lx * lx + lz * lz) - tp * tp;
   if (qm_below_neg_eps(tp) || delta > r2) return false;
-  const float s = r2 - delta;
-  const float t_plus = delta <= 0.0f ? r.size.x : s * rsqrtf(s);
+  const float s = r2 - delta;  // >= 0 here; 0 for a ray grazing the silhouette
+  const float t_plus = delta <= 0.0f ? r.size.x : (s > 0.0f ? s * rsqrtf(s) : 0.0f);
   t = (tp - t_plus) * il;
   const float3 ip = make_float3(d.x * t + o.x, d.y * t + o.y, d.z * t + o.z);
   u = __fdividef(ip.y - r.pos.y, r.size.y) + 0.5f;

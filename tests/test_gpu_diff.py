@@ -260,8 +260,8 @@ def test_adjoint_on_a_slice_of_the_benchmark_field(tmp_path, cuda_device):
     cylinder image, Gaussian splat sigma 2 px, a smooth seeded target with
     peak/mean <= 2, aim offsets U(+-1 m) and normal offsets U(+-1 mrad),
     central differences at h = 1e-3 m / 1e-5 rad under common random numbers
-    (the scene's fixed pools and facet offsets), 64 light indexes per facet
-    (0.92 G rays per forward, so the float rounding of the traced rays that
+    (the scene's fixed pools and facet offsets), 256 light indexes per facet
+    (3.7 G rays per forward, so the float rounding of the traced rays that
     the differences also difference averages out).
 
     Bars (written here): relative 2-norm error of the adjoint per parameter
@@ -276,7 +276,7 @@ def test_adjoint_on_a_slice_of_the_benchmark_field(tmp_path, cuda_device):
     H = s.num_heliostats
     assert H == 48 and s.heliostat(0)["num_facets"] == 300664
     d = q.Diff(s, 2.0)
-    d.set_light_range(0, 64)
+    d.set_light_range(0, 256)
     shape = (s.receiver(0)["height"], s.receiver(0)["width"])
     d.set_target(np.zeros(shape, np.float32))
     d.forward()
