@@ -109,8 +109,9 @@ def accuracy(scene_path: str, config_path: str, path: str) -> dict:
     for k, h in enumerate(rec_ids):
         h, fb = int(h), int(rec_fb[k])
         o1 = scene_offsets(f32, seed, [h])
-        want = f32.trace([h], dirs, pert, o1, 0, rl, record=(h, fb, fb + nfac), images=False)["records"]
-        w64 = f64.trace([h], dirs, pert, o1, 0, rl, record=(h, fb, fb + nfac), images=False)["records"]
+        rec = (h, fb, fb + nfac)
+        want = f32.trace([h], dirs, pert, o1, 0, rl, record=rec, images=False, record_only=True)["records"]
+        w64 = f64.trace([h], dirs, pert, o1, 0, rl, record=rec, images=False, record_only=True)["records"]
         got = codes[k]
         n += got.size
         same += int(np.count_nonzero(got == want))

@@ -47,7 +47,7 @@ class TraceArgs(ctypes.Structure):
         ("offsets", _pi), ("offset_base", _pll), ("light_begin", _i), ("light_end", _i),
         ("facet_stride", _i), ("facet_phase", _i), ("images", _pd), ("image_base", _pll), ("power", _pd),
         ("counters", _pll), ("rec_id", _i), ("rec_facet_begin", _i), ("rec_facet_end", _i), ("records", _pi),
-        ("threads", _i),
+        ("threads", _i), ("record_only", _i),
     ]
 
 
@@ -227,10 +227,12 @@ class OracleScene:
         return bool(lib().oracle_walk(self.h, grid, own_begin, own_n, _p(o, _d), _p(d, _d)))
 
     def trace(self, ids, pool_dirs, pool_pert, offsets, light_begin=0, light_end=None, facet_stride=1,
-              facet_phase=0, images=True, record=None, threads=0):
+              facet_phase=0, images=True, record=None, threads=0, record_only=False):
         """Trace heliostats `ids`.  offsets: dict heliostat -> int array of
         num_facets + 1.  record = (heliostat, facet_begin, facet_end) returns
-        per-ray codes.  Returns dict(images=[per receiver 2D], power, counters, records)."""
+        per-ray codes; with record_only that heliostat traces only the
+        recorded facets (images, powers and counters then cover just those).
+        Returns dict(images=[per receiver 2D], power, counters, records)."""
         ids = np.ascontiguousarray(np.array(ids, np.int32))
         P = self.pool_size
         dirs = np.ascontiguousarray(np.asarray(pool_dirs, np.float32).reshape(P, 3))
@@ -283,6 +285,7 @@ class OracleScene:
             a.rec_id, a.rec_facet_begin, a.rec_facet_end = -1, 0, 0
             a.records = None
         a.threads = threads
+        a.record_only = 1 if (record is not None and record_only) else 0
         lib().oracle_trace(self.h, ctypes.byref(a))
         images_out = []
         for r, rc in enumerate(recs):

@@ -565,6 +565,7 @@ struct TraceArgs {
   int rec_id, rec_facet_begin, rec_facet_end;
   int* records;
   int threads;
+  int record_only;            // with records: trace only heliostat rec_id's facets [rec_facet_begin, rec_facet_end)
 };
 
 template <class T>
@@ -590,8 +591,11 @@ void trace(const Scene<T>& s, const TraceArgs& a) {
       const Recv<T>& r = s.recv[g.recv];
       const int* off = a.offsets + a.offset_base[hid];
       const T factor = s.factor[hid];
+      const bool only = a.records && a.record_only && hid == a.rec_id;
+      const int f_begin = only ? std::max(0, a.rec_facet_begin) : 0;
+      const int f_end = only ? std::min(h.n_facets, a.rec_facet_end) : h.n_facets;
 #pragma omp for schedule(dynamic, 64) nowait
-      for (int f = 0; f < h.n_facets; ++f) {
+      for (int f = f_begin; f < f_end; ++f) {
         if (a.facet_stride > 1 && f % a.facet_stride != a.facet_phase) continue;
         V<T> o, n0;
         facet(h, f, o, n0);

@@ -82,8 +82,10 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
         assert nf == 300664
         fb = int(rng.integers(0, nf - 2000))
         fe = fb + 2000
-        want = host.trace([h], dirs, pert, offsets, record=(h, fb, fe), images=False)["records"]
-        ref64 = fp64.trace([h], dirs, pert, offsets, record=(h, fb, fe), images=False)["records"]
+        want = host.trace([h], dirs, pert, offsets, record=(h, fb, fe), images=False,
+                          record_only=True)["records"]
+        ref64 = fp64.trace([h], dirs, pert, offsets, record=(h, fb, fe), images=False,
+                           record_only=True)["records"]
         s.set_math_mode(1)
         exact = s.hit_records(h, fb, fe, 0, L)
         diff = exact != want
