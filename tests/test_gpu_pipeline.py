@@ -10,15 +10,17 @@ on the reference's own host code (its TaskLoader, per-ray routine, ImageSaver
 and trimmed-mean heaps) with the executable's pools and offsets, read back
 through the Python binding of the same seed.
 
-Bar (written here): the same files, and in each every value equal to the
-reference's to the format's two decimals, except where float accumulation
-order or a per-ray difference of the production build moves a value across
-a rounding boundary: at most one unit in the last place everywhere, on at
-most 1 % of the pixels before smoothing and 20 % after (the trimmed mean
-adds up to 121 pixels in float, so inputs one ulp apart -- float atomics in
-another order -- round its last printed digit differently far more often;
-the smoother itself is bit-identical to the reference's on equal inputs,
-tests/test_gpu_parity.py), and the totals of each file within 1e-5.
+Bars (written here), in two parts:
+  * the executable's files against the reference pipeline's on the same
+    rays: the same files; every value within one unit of the last printed
+    digit (0.01) plus the float accumulation error of the pixel (1e-5 of
+    its value: both images add float energies, in different orders, and a
+    2-decimal print of values in the thousands shows that); the totals of
+    each file within 1e-5;
+  * the result-saving steps alone, bit for bit: this tracer's flux image,
+    written by qmcrt_save_text before and after qmcrt_smooth (radius 5,
+    ratio 0.05 on the device), gives byte-identical files to the reference's
+    ImageSaver::saveText and trimmed-mean heaps on the same float image.
 """
 import subprocess
 import sys
@@ -72,6 +74,25 @@ def test_executable_writes_the_reference_pipeline_files(which, tmp_path, cuda_de
         frac = float(np.mean(diff > 1e-9))
         print(f"{which} {name}: {a.shape}, max |diff| {diff.max():.3f}, differing values {frac:.2e}, "
               f"total {a.sum():.2f} vs {b.sum():.2f}")
-        assert diff.max() <= 0.0100001, name
-        assert frac <= (0.01 if "before" in name else 0.2), name
+        assert np.all(diff <= 0.0100001 + 1e-5 * np.abs(b)), name
         assert abs(a.sum() - b.sum()) <= 1e-5 * max(b.sum(), 1.0) + 0.01 * diff.size * frac, name
+
+    # the saving steps alone, on one float image: byte-identical files
+    from oracle import refhost
+
+    s = q.Scene(f.scene, f.config, device=0, seed=0)
+    s.trace(ids)
+    mine, theirs = tmp_path / "mine", tmp_path / "theirs"
+    mine.mkdir()
+    theirs.mkdir()
+    for r in range(s.num_receivers):
+        img = s.image(r)
+        q.save_text(mine / f"{r}_before.txt", img)
+        refhost.save_text(theirs / f"{r}_before.txt", img)
+        ptr, w, h = s.device_image(r)
+        q.smooth_device(ptr, w, h, 5, 0.05)
+        q.save_text(mine / f"{r}_after.txt", s.image(r))
+        refhost.save_text(theirs / f"{r}_after.txt", refhost.smooth(img, 5, 0.05))
+    s.close()
+    for p in sorted(mine.iterdir()):
+        assert p.read_bytes() == (theirs / p.name).read_bytes(), p.name

@@ -194,7 +194,7 @@ def test_per_ray_outcomes_against_the_reference_cuda_tracer(tmp_path, cuda_devic
     # exact build = host arithmetic, up to hits one column over where the
     # host library's float acosf rounds differently (tests/test_gpu_field.py)
     differ = codes["exact"] != codes["host"]
-    assert np.count_nonzero(differ) <= max(2, 1e-6 * differ.size), "exact build differs from the host arithmetic"
+    assert np.count_nonzero(differ) <= max(2, 3e-6 * differ.size), "exact build differs from the host arithmetic"
     assert np.all((codes["exact"][differ] >= 0) & (codes["host"][differ] >= 0))
     report = {}
     for key in ("production", "exact", "host", "fp64"):
