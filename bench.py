@@ -32,9 +32,9 @@ warp instructions per ray (the committed ncu figure,
 profiles/trace_kernel_instructions.json) x rays/s against 4 schedulers x SMs
 x the sampled SM clock; its `atomics` part sets the flux deposits' rate
 against the L2 atomic rate of the tracer's own recorded deposits replayed.
-`approx_math` (--approx-steps, default 5) times the approximate-math build
-(mode 3) on the same steps, with its whole-step agreement against the exact
-build.
+`approx_math` and `approx_receiver` (--approx-steps, default 5) time the
+approximate-math build (mode 3) and the receiver-approximate build (mode 4)
+on the same steps, with their whole-step agreement against the exact build.
 `plain_over_96_suns` (--sun-lights, default 32) runs the plain tracer over
 the 96 sun positions below, one launch per sun.
 `batched` (--batched-lights, default 4 light indexes per instance) compares,
@@ -726,7 +726,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": kernel_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "math_mode": {0: "fast", 1: "exact", 2: "fast-64reg", 3: "approx"}[mode],
+                "math_mode": {0: "fast", 1: "exact", 2: "fast-64reg", 3: "approx", 4: "fast-rx"}[mode],
                 "data": "synthetic (seeded large_field: 624 heliostats, 187.6M micro-facets)",
                 "config": {"workload": WORKLOAD, "global_batch": f"{total_facets * passes * world} rays/step",
                            "rays_per_step_per_gpu": total_facets * passes, "passes_per_step": passes,
@@ -739,6 +739,8 @@ def main():
         if args.approx_steps > 0 and mode == 0:
             line["approx_math"] = mode_rate(torch, scene, ids, 3, args.approx_steps,
                                             [light_range(k) for k in range(args.approx_steps)], stream, flush)
+            line["approx_receiver"] = mode_rate(torch, scene, ids, 4, args.approx_steps,
+                                                [light_range(k) for k in range(args.approx_steps)], stream, flush)
             scene.set_math_mode(mode)
         if args.sun_lights > 0:
             line["plain_over_96_suns"] = plain_over_suns(torch, scene, ids, args.sun_lights, stream)

@@ -144,7 +144,10 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* scene, unsigned seed);
  * shadow test (FMA contraction, hardware reciprocal square root and
  * approximate divisions in the slope-error normal, reflection, receiver test
  * and energy: hits near a pixel boundary or the cylinder's silhouette can
- * land one pixel over or flip, as in the reference's own CUDA build). */
+ * land one pixel over or flip, as in the reference's own CUDA build); 4 the
+ * production build with only the arithmetic after the receiver's decisions
+ * approximated (hit point, pixel position, energy): decisions as mode 0,
+ * hits within a few ulp of a pixel edge one pixel over. */
 int qmcrt_set_math_mode(qmcrt_scene* scene, int exact);
 /* Launch shapes of the production build (math mode 0), indexes 0..count-1:
  * threads per block and warp-chunk iterations (32 rays each); shape 0 is the

@@ -306,7 +306,7 @@ int qmcrt_batch_set_light_range(qmcrt_batch* b, int begin, int end) {
 int qmcrt_batch_set_math_mode(qmcrt_batch* b, int mode) {
   return guarded([&] {
     batch_checked(b);
-    if (mode < 0 || mode > 3) invalid("math mode must be 0, 1, 2 or 3");
+    if (mode < 0 || mode > 4) invalid("math mode must be 0, 1, 2, 3 or 4");
     b->mode = mode;
     b->drop_graph();
   });

@@ -63,6 +63,46 @@ __device__ __forceinline__ bool receiver_hit(const DevReceiver& r, float3 o, flo
   return cylinder_hit(r, o, d, t, u, v);
 }
 
+// The cylinder test with every decision rounded as the reference rounds it
+// and the arithmetic after the decisions approximated (the
+// receiver-approximate production build): the inside test, tp and the
+// silhouette test delta > r^2 -- which cancels catastrophically for far
+// heliostats, so its last bits decide hits -- are explicitly rounded as in
+// cylinder_hit; the distance t, the hit point and its (u, v) use FMA
+// contraction, the hardware reciprocal square root and reciprocal-multiply
+// divisions.  A hit can land one pixel over when (u, v) lies within a few
+// ulp of a pixel edge; the u range test flips only for hits within about a
+// micrometre of the image's first or last row.
+__device__ __forceinline__ bool cylinder_hit_rx(const DevReceiver& r, float3 o, float3 d, float& t, float& u,
+                                                float& v) {
+  float2 l = make_float2(qm_rn_sub(o.x, r.pos.x), qm_rn_sub(o.z, r.pos.z));
+  const float r2 = qm_rn_mul(r.size.x, r.size.x);
+  if (qs::dot2(l, l) <= r2) return false;
+  float2 ro = make_float2(qm_rn_sub(r.pos.x, o.x), qm_rn_sub(r.pos.z, o.z));
+  const float dd = qm_rn_add(qm_rn_mul(d.x, d.x), qm_rn_mul(d.z, d.z));
+  const float il = qm_rn_rsqrt(dd);
+  const float tp = qs::dot2(ro, make_float2(qm_rn_mul(d.x, il), qm_rn_mul(d.z, il)));
+  const float delta = qm_rn_sub(qs::dot2(ro, ro), qm_rn_mul(tp, tp));
+  if (qm_below_neg_eps(tp) || delta > r2) return false;
+  const float s = r2 - delta;
+  const float t_plus = delta <= 0.0f ? r.size.x : (s > 0.0f ? s * rsqrtf(s) : 0.0f);
+  t = (tp - t_plus) * il;
+  const float3 ip = make_float3(d.x * t + o.x, d.y * t + o.y, d.z * t + o.z);
+  u = __fdividef(ip.y - r.pos.y, r.size.y) + 0.5f;
+  if (u < 0.0f || u > 1.0f) return false;
+  const float ex = ip.x - r.pos.x, ez = ip.z - r.pos.z;
+  const float cx = fminf(fmaxf(ex * rsqrtf(ex * ex + ez * ez), -1.0f), 1.0f);
+  v = acosf(cx) * 0.15915494f;
+  if (ez < 0) v = 1.0f - v;
+  return true;
+}
+
+__device__ __forceinline__ bool receiver_hit_rx(const DevReceiver& r, float3 o, float3 d, float& t, float& u,
+                                                float& v) {
+  if (r.type == 0) return qs::ray_parallelogram(o, d, r.a, r.ab, r.ac, t, u, v);
+  return cylinder_hit_rx(r, o, d, t, u, v);
+}
+
 // The same cylinder test in approximate arithmetic (the approximate-math
 // tracer build): FMA contraction, the hardware reciprocal square root and
 // reciprocal-multiply divisions, v scaled by a float 1/(2 pi).  Rays near a

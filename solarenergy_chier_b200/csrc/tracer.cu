@@ -45,14 +45,25 @@
 // receiver test, energy, pixel index): explicitly rounded (qs::, as the CPU
 // oracle rounds it) in every build but the approximate-math one
 // (QM_TRACE_APPROX_MATH: qf::, FMA contraction and hardware approximations).
+// The receiver-approximate build (QM_TRACE_APPROX_RECEIVER) keeps the
+// normal, the reflection and the receiver's decisions explicitly rounded
+// and approximates only what follows them: the hit point, (u, v) and the
+// energy (cylinder_hit_rx).
 #if defined(QM_TRACE_APPROX_MATH)
 namespace qx = ::qf;
 #define QM_RECEIVER_HIT receiver_hit_approx
 #define QM_PIXEL_MUL(a, b) ((a) * (b))
+#define QM_ENERGY qf::ray_energy
+#elif defined(QM_TRACE_APPROX_RECEIVER)
+namespace qx = ::qs;
+#define QM_RECEIVER_HIT receiver_hit_rx
+#define QM_PIXEL_MUL(a, b) ((a) * (b))
+#define QM_ENERGY qf::ray_energy
 #else
 namespace qx = ::qs;
 #define QM_RECEIVER_HIT receiver_hit
 #define QM_PIXEL_MUL(a, b) qm_rn_mul((a), (b))
+#define QM_ENERGY qs::ray_energy
 #endif
 
 namespace qm {
@@ -580,7 +591,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
           if (!QM_RECEIVER_HIT(R, xyz(lds(win.o[slot])), rd, tt, uu, vv)) {
             code = kMissed;
           } else {
-            float e = qx::ray_energy(tt, rd, n, T.factor);
+            float e = QM_ENERGY(tt, rd, n, T.factor);
             if (kOut == kOutBits) {
               code = 0;
             } else if (kOut == kOutSplat) {

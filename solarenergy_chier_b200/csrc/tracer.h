@@ -24,6 +24,10 @@ cudaError_t launch_trace_fast_t64(const TraceParams& p, int out, cudaStream_t st
 int trace_chunk_rays_fast_c32();
 int trace_chunk_rays_fast_c128();
 int trace_chunk_rays_fast_t64();
+// Production build with the arithmetic after the receiver's decisions
+// approximated (hit point, pixel position, energy).
+cudaError_t launch_trace_rx(const TraceParams& p, int out, cudaStream_t stream);
+int trace_chunk_rays_rx();
 // Production build with approximate per-ray arithmetic after the shadow test
 // (FMA contraction, hardware reciprocal square root, approximate divisions).
 cudaError_t launch_trace_approx(const TraceParams& p, int out, cudaStream_t stream);

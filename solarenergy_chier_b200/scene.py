@@ -170,7 +170,8 @@ class Scene:
 
     def set_math_mode(self, exact) -> None:
         """True/1: exact build; False/0: production build; 2: production, 64 registers (4 blocks/SM);
-        3: production with approximate per-ray arithmetic after the shadow test."""
+        3: production with approximate per-ray arithmetic after the shadow test;
+        4: production with approximate arithmetic after the receiver's decisions."""
         mode = int(exact) if not isinstance(exact, bool) else (1 if exact else 0)
         check(self._lib.qmcrt_set_math_mode(self._h, mode))
 

@@ -33,6 +33,9 @@ Bars (the north star's, written here):
     (below); against the exact build on the whole step its distance is
     reported with outer bounds (decisions 1e-3, flux L1 1e-2, power 1e-3;
     measured 4.5e-4, 4.9e-3, 2.0e-4);
+  * the receiver-approximate build (mode 4) meets the production bars
+    (decisions >= 99.99 %, outcomes >= 99.9 %, whole step 1e-4 / 1e-3 /
+    1e-5);
   * FP64: on the same 48 heliostats x every facet x light indexes 0-7
     (115 M rays) the flux's L1 distance and total-power error from the FP64
     oracle are measured beside the host arithmetic's own, for the production
@@ -79,6 +82,7 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
     prod_vs_fp64 = host_vs_fp64 = 0
     approx_dec = approx_same = approx_vs_fp64 = 0
     exact_shift = 0
+    rx_dec = rx_same = 0
     W = s.receiver(0)["width"]
     for h in ids:
         nf = s.heliostat(h)["num_facets"]
@@ -103,6 +107,10 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
         approx_dec += int(np.count_nonzero((approx >= 0) == (want >= 0)))
         approx_same += int(np.count_nonzero(approx == want))
         approx_vs_fp64 += int(np.count_nonzero((approx >= 0) != (ref64 >= 0)))
+        s.set_math_mode(4)
+        rx = s.hit_records(h, fb, fe, 0, L)
+        rx_dec += int(np.count_nonzero((rx >= 0) == (want >= 0)))
+        rx_same += int(np.count_nonzero(rx == want))
         s.set_math_mode(0)
         got = s.hit_records(h, fb, fe, 0, L)
         n += got.size
@@ -114,15 +122,17 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
         {"rays": n, "decision_agreement": prod_dec / n, "outcome_agreement": prod_same / n,
          "exact_build_column_shifts": exact_shift / n,
          "approx_math": {"decision_agreement": approx_dec / n, "outcome_agreement": approx_same / n},
+         "approx_receiver": {"decision_agreement": rx_dec / n, "outcome_agreement": rx_same / n},
          "decision_flips_vs_fp64": {"production": prod_vs_fp64 / n, "host_arithmetic": host_vs_fp64 / n,
                                     "approx_math": approx_vs_fp64 / n}}))
     assert exact_shift <= 3e-6 * n
     assert prod_dec >= 0.9999 * n
     assert prod_same >= 0.999 * n
     assert approx_vs_fp64 <= host_vs_fp64 + 1e-5 * n
+    assert rx_dec >= 0.9999 * n and rx_same >= 0.999 * n
 
 
-@pytest.mark.parametrize("mode", [0, 3])
+@pytest.mark.parametrize("mode", [0, 3, 4])
 def test_whole_field_step_against_the_exact_build(field, mode):
     import torch
 
@@ -154,13 +164,13 @@ def test_whole_field_step_against_the_exact_build(field, mode):
     print(f"bench step, mode {mode} vs exact build:", json.dumps(report))
     s.set_light_range(0, s.lights_per_group)
     s.set_math_mode(0)
-    bars = (1e-4, 1e-3, 1e-5) if mode == 0 else (1e-3, 1e-2, 1e-3)
+    bars = (1e-3, 1e-2, 1e-3) if mode == 3 else (1e-4, 1e-3, 1e-5)
     assert flips <= bars[0] * rays
     assert report["flux_l1"] <= bars[1]
     assert report["power_rel"] <= bars[2]
 
 
-@pytest.mark.parametrize("mode", [0, 3])
+@pytest.mark.parametrize("mode", [0, 3, 4])
 def test_error_against_fp64_on_the_benchmark_field(field, mode):
     files, s, dirs, pert, ids, offsets = field
     lights = 8
@@ -184,7 +194,7 @@ def test_error_against_fp64_on_the_benchmark_field(field, mode):
               "power_rel_vs_fp64": abs(total - t64) / t64, "host_arithmetic_power_rel_vs_fp64": abs(t32 - t64) / t64,
               "power_rel_vs_host_arithmetic": abs(total - t32) / t32}
     print(f"FP64 on the benchmark field, mode {mode}:", json.dumps(report))
-    if mode == 0:
+    if mode != 3:
         assert report["flux_l1_vs_host_arithmetic"] <= 1e-3
         assert report["power_rel_vs_host_arithmetic"] <= 1e-5
     assert report["flux_l1_vs_fp64"] <= 1.05 * report["host_arithmetic_flux_l1_vs_fp64"] + 1e-4
