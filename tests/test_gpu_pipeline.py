@@ -12,11 +12,16 @@ through the Python binding of the same seed.
 
 Bars (written here), in two parts:
   * the executable's files against the reference pipeline's on the same
-    rays: the same files; every value within one unit of the last printed
-    digit (0.01) plus the float accumulation error of the pixel (1e-5 of
-    its value: both images add float energies, in different orders, and a
-    2-decimal print of values in the thousands shows that); the totals of
-    each file within 1e-5;
+    rays: the same files; every value before smoothing within one unit of
+    the last printed digit (0.01) plus the float accumulation error of the
+    pixel (1e-5 of its value: both images add float energies, in different
+    orders, and a 2-decimal print of values in the thousands shows that);
+    after smoothing the same on all but 1 % of the pixels (the reference's
+    streaming trimmed mean, radius 5, keeps six values a side in heaps fed
+    in window order and is not a sorted trim: one comparison between two
+    nearly equal inputs that float rounding decides the other way changes
+    which values the heaps end up holding, and the mean by up to about 1 %);
+    the totals of each file within 1e-5;
   * the result-saving steps alone, bit for bit: this tracer's flux image,
     written by qmcrt_save_text before and after qmcrt_smooth (radius 5,
     ratio 0.05 on the device), gives byte-identical files to the reference's
@@ -74,7 +79,11 @@ def test_executable_writes_the_reference_pipeline_files(which, tmp_path, cuda_de
         frac = float(np.mean(diff > 1e-9))
         print(f"{which} {name}: {a.shape}, max |diff| {diff.max():.3f}, differing values {frac:.2e}, "
               f"total {a.sum():.2f} vs {b.sum():.2f}")
-        assert np.all(diff <= 0.0100001 + 1e-5 * np.abs(b)), name
+        within = diff <= 0.0100001 + 1e-5 * np.abs(b)
+        if "before" in name:
+            assert np.all(within), name
+        else:
+            assert np.mean(~within) <= 0.01, name
         assert abs(a.sum() - b.sum()) <= 1e-5 * max(b.sum(), 1.0) + 0.01 * diff.size * frac, name
 
     # the saving steps alone, on one float image: byte-identical files
