@@ -47,7 +47,7 @@ its adjoint (aim-point optimisation set-up) on the field.
 `large_adjoint` (--large-adjoint-lights N, default 4; 0 = skipped) times one
 forward + adjoint over 32 suns of a 10,000-heliostat field (its rays'
 errors against FP64 on a 1 % subsample: tests/test_gpu_diff.py).
-`aim_optimisation` (--adam-steps K, default 0 = skipped) runs K Adam steps
+`aim_optimisation` (--adam-steps K, default 200; 0 = skipped) runs K Adam steps
 of aim-point optimisation on the field's 624 x 2 aim offsets, each step
 checked by the plain tracer on the same parameters.
 The reference's own CUDA build is timed beside this tracer by
@@ -95,7 +95,7 @@ def parse_args():
                    help="light indexes per sun of the plain tracer looped over the 96 suns (0 = skip)")
     p.add_argument("--batched-lights", type=int, default=4,
                    help="light indexes per sun of the 96-sun batched-vs-plain comparison (0 = skip)")
-    p.add_argument("--adam-steps", type=int, default=0,
+    p.add_argument("--adam-steps", type=int, default=200,
                    help="Adam steps of aim-point optimisation, each checked by the plain tracer (0 = skip)")
     p.add_argument("--adam-lights", type=int, default=8, help="light indexes per facet of each Adam step")
     p.add_argument("--large-adjoint-lights", type=int, default=4,
