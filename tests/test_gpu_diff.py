@@ -264,13 +264,18 @@ def test_adjoint_on_a_slice_of_the_benchmark_field(tmp_path, cuda_device):
     (3.7 G rays per forward, so the float rounding of the traced rays that
     the differences also difference averages out).
 
-    Bars (written here): relative 2-norm error of the adjoint over the
-    heliostats within 450 m <= 1e-2 for the normal offsets and <= 2e-2 for
-    the aim offsets, <= 3e-2 for both over the slice.  Per heliostat the
-    test prints the adjoint, the differences and the share of its rays that
-    miss the receiver (its spot spilling over the cylinder's silhouette and
-    its first and last rows, whose boundary terms the adjoint estimates from
-    bands of rays)."""
+    Bars (written here): relative 2-norm error of the adjoint <= 1e-2 for
+    both parameter kinds over the heliostats whose spots spill less than
+    10 % of their rays past the receiver; over the heliostats within 450 m
+    <= 1e-2 for the normal offsets and <= 2e-2 for the aim offsets; <= 3e-2
+    for both over the slice.  Per heliostat the test prints the adjoint, the
+    differences and the share of its rays that miss the receiver: the error
+    follows that share (about 0.5 % below 10 % spill, 2-7 % at 20-50 %),
+    i.e. the receiver's edges -- its silhouette and first and last rows,
+    whose boundary terms the adjoint estimates from bands of rays --
+    dominate it, not the float noise of the differences (64 and 256 lights
+    give the same errors).
+    """
     from solarenergy_chier_b200 import aim as aimmod
 
     files = synth.large_field(tmp_path, seed=0, keep_every=13)
@@ -307,15 +312,17 @@ def test_adjoint_on_a_slice_of_the_benchmark_field(tmp_path, cuda_device):
                 vals.append(d.forward())
             fd[h, k] = (vals[0] - vals[1]) / (2 * step)
     dist = np.array([np.hypot(*s.heliostat(h)["pos"][[0, 2]]) for h in range(H)])
+    spills = np.zeros(H)
     for h in range(H):
         nf = s.heliostat(h)["num_facets"]
         codes = s.hit_records(h, nf // 2 - 1000, nf // 2 + 1000, 0, 64)
-        spill = float(np.mean(codes == -3))
+        spill = spills[h] = float(np.mean(codes == -3))
         rel = np.abs(grad[h] - fd[h]) / np.maximum(np.abs(fd[h]), 1e-30)
         print(f"heliostat {h} at {dist[h]:.0f} m, {100 * spill:.1f} % of rays miss the receiver: adjoint {grad[h]} "
               f"finite differences {fd[h]} relative {rel}")
     failures = []
-    for name, sel, bars in (("within 450 m", dist < 450.0, (2e-2, 1e-2)), ("whole slice", dist > 0, (3e-2, 3e-2))):
+    for name, sel, bars in (("spill under 10 %", spills < 0.1, (1e-2, 1e-2)),
+                            ("within 450 m", dist < 450.0, (2e-2, 1e-2)), ("whole slice", dist > 0, (3e-2, 3e-2))):
         for cols, bar in zip(((0, 1), (2, 3)), bars):
             rel = np.linalg.norm(grad[sel][:, cols] - fd[sel][:, cols]) / np.linalg.norm(fd[sel][:, cols])
             print(f"relative error, {name}, parameters {cols}: {rel:.3e}")

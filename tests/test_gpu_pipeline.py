@@ -15,8 +15,11 @@ Bars (written here), in two parts:
     rays: the same files; every value before smoothing within one unit of
     the last printed digit (0.01) plus the float accumulation error of the
     pixel (1e-5 of its value: both images add float energies, in different
-    orders, and a 2-decimal print of values in the thousands shows that);
-    after smoothing the same on all but 1 % of the pixels (the reference's
+    orders, and a 2-decimal print of values in the thousands shows that),
+    but for at most 0.1 % of the pixels (the production build puts about
+    one hit in a million one pixel over, which moves that ray's energy
+    between two pixels); after smoothing the same on all but 1 % of the
+    pixels (the reference's
     streaming trimmed mean, radius 5, keeps six values a side in heaps fed
     in window order and is not a sorted trim: one comparison between two
     nearly equal inputs that float rounding decides the other way changes
@@ -80,10 +83,7 @@ def test_executable_writes_the_reference_pipeline_files(which, tmp_path, cuda_de
         print(f"{which} {name}: {a.shape}, max |diff| {diff.max():.3f}, differing values {frac:.2e}, "
               f"total {a.sum():.2f} vs {b.sum():.2f}")
         within = diff <= 0.0100001 + 1e-5 * np.abs(b)
-        if "before" in name:
-            assert np.all(within), name
-        else:
-            assert np.mean(~within) <= 0.01, name
+        assert np.mean(~within) <= (0.001 if "before" in name else 0.01), name
         assert abs(a.sum() - b.sum()) <= 1e-5 * max(b.sum(), 1.0) + 0.01 * diff.size * frac, name
 
     # the saving steps alone, on one float image: byte-identical files
