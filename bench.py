@@ -726,7 +726,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": kernel_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "math_mode": {0: "fast", 1: "exact", 2: "fast-64reg", 3: "approx", 4: "fast-rx", 5: "fast-prefetch"}[mode],
+                "math_mode": {0: "fast", 1: "exact", 2: "fast-64reg", 3: "approx", 4: "fast-rx"}[mode],
                 "data": "synthetic (seeded large_field: 624 heliostats, 187.6M micro-facets)",
                 "config": {"workload": WORKLOAD, "global_batch": f"{total_facets * passes * world} rays/step",
                            "rays_per_step_per_gpu": total_facets * passes, "passes_per_step": passes,

@@ -51,8 +51,6 @@ CUDA_UNITS = [
                                             "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_fast_t64.o", ["-DQM_TRACE_VARIANT=fast_t64", "-DQM_TRACE_THREADS=64", "-DQM_TRACE_MIN_BLOCKS=14",
                                            "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS"]),
-    ("tracer.cu", "tracer_fast_pf.o", ["-DQM_TRACE_VARIANT=fast_pf", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
-                                          "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS", "-DQM_TRACE_PREFETCH"]),
     ("tracer.cu", "tracer_rx.o", ["-DQM_TRACE_VARIANT=rx", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
                                      "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS", "-DQM_TRACE_APPROX_RECEIVER"]),
     ("tracer.cu", "tracer_approx.o", ["-DQM_TRACE_VARIANT=approx", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",

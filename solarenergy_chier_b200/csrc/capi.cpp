@@ -463,7 +463,6 @@ cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaS
     case 2: e = qm::launch_trace_fast4(p, out, st); break;
     case 3: e = qm::launch_trace_approx(p, out, st); break;
     case 4: e = qm::launch_trace_rx(p, out, st); break;
-    case 5: e = qm::launch_trace_fast_pf(p, out, st); break;
     default: e = kShapes[shape_for(mode, shape, out)].launch(p, out, st); break;
   }
   // flux and bilinear-deposit launches add their per-chunk power partials
@@ -852,7 +851,7 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* s, unsigned seed) {
 
 int qmcrt_set_math_mode(qmcrt_scene* s, int exact) {
   return guarded([&] {
-    if (exact < 0 || exact > 5)
+    if (exact < 0 || exact > 4)
       invalid("math mode must be 0 (production), 1 (exact), 2 (production, 64 registers), 3 (approximate math) or "
               "4 (production, approximate receiver arithmetic)");
     checked(s)->exact = exact;

@@ -505,29 +505,9 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   unsigned long long clamped = 0;
   int base = 0;        // first facet id of the window
   bool filled = false;  // warp-uniform
-#if defined(QM_TRACE_PREFETCH)
-  // Software pipelining of the sun-shape sample: each iteration loads the
-  // next iteration's sample (its facet's pool offset read from the task's
-  // offset array, which the window caches) before its own work, so the L2
-  // latency of that load overlaps a whole ray's arithmetic.
-  float4 dir_next = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (r0 + lane < r_end) dir_next = __ldg(T.samples + __ldg(T.offsets + f) + p.light_begin + l);
-#endif
   for (int it = 0; it < iters; ++it) {
     const bool active = r0 + it * 32 + lane < r_end;
     bool hit = false;
-#if defined(QM_TRACE_PREFETCH)
-    const float4 dir_now = dir_next;
-    {
-      int fn = f + q32, ln = l + r32;
-      if (ln >= nl) {
-        ln -= nl;
-        ++fn;
-      }
-      if (it + 1 < iters && r0 + (it + 1) * 32 + lane < r_end)
-        dir_next = __ldg(T.samples + __ldg(T.offsets + fn) + p.light_begin + ln);
-    }
-#endif
     // Lane 0 holds the smallest facet of the iteration (it is active whenever
     // any lane is) and every facet of the iteration lies within 31 of it.
     const int f0 = __shfl_sync(0xffffffffu, f, 0);
@@ -571,11 +551,7 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
       // P + L entries (entry P + i repeats entry i), so (g + l) % P needs no
       // modulo.  The sun-shape pool is stored already turned by the sun
       // frame (world space).
-#if defined(QM_TRACE_PREFETCH)
-      const float3 dir = xyz(dir_now);
-#else
       const float3 dir = xyz(__ldg(lds_ptr(win.samples[threadIdx.x >> 5]) + __float_as_int(win.o[slot].w) + lab));
-#endif
       int32_t code;
       // Heliostats whose rays no other heliostat can shadow skip the shadow
       // walk; where only a few listed heliostats can (qm::cone_candidates,

@@ -28,8 +28,6 @@ int trace_chunk_rays_fast_t64();
 // approximated (hit point, pixel position, energy).
 cudaError_t launch_trace_rx(const TraceParams& p, int out, cudaStream_t stream);
 int trace_chunk_rays_rx();
-// Production build with the sun-shape sample of the next iteration loaded ahead.
-cudaError_t launch_trace_fast_pf(const TraceParams& p, int out, cudaStream_t stream);
 // Production build with approximate per-ray arithmetic after the shadow test
 // (FMA contraction, hardware reciprocal square root, approximate divisions).
 cudaError_t launch_trace_approx(const TraceParams& p, int out, cudaStream_t stream);
