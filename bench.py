@@ -103,6 +103,7 @@ def parse_args():
     p.add_argument("--impl", default="native", choices=["native", "reference"])
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="keep launch shape 0 instead of autotuning it")
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target length of the CPU baseline sample")
     p.add_argument("--exact", action="store_true", help="time the kernel build without FMA contraction")
     p.add_argument("--mode", type=int, default=None, help="kernel build: 0 production, 1 exact, 2 production at 4 blocks/SM")
@@ -620,6 +621,14 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    # ---- launch shape: the autotuner times the production build's shapes on
+    # the step's heliostats and light range and keeps the fastest ---------------
+    tuned = None
+    if mode == 0 and not args.no_autotune:
+        scene.set_light_range(*light_range(0))
+        best, shape_ms = scene.autotune(ids, stream)
+        tuned = {"chosen": best, "shapes": q.launch_shapes(), "ms_per_shape": shape_ms}
+
     # ---- device-resident throughput -------------------------------------------
     for step in range(args.warmup):
         scene.set_light_range(*light_range(step))
@@ -731,7 +740,7 @@ def main():
                 "config": {"workload": WORKLOAD, "global_batch": f"{total_facets * passes * world} rays/step",
                            "rays_per_step_per_gpu": total_facets * passes, "passes_per_step": passes,
                            "seq_len": None, "parallelism": f"weak x{world} (light-index shards)",
-                           "l2": "flushed before every step (256 MB write)"},
+                           "l2": "flushed before every step (256 MB write)", "launch_shape": tuned},
                 "wall_s": wall, "clocks": clocks, "gpu_launches": args.steps,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps},

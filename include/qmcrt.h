@@ -150,11 +150,13 @@ int qmcrt_generate_facet_offsets(qmcrt_scene* scene, unsigned seed);
  * hits within a few ulp of a pixel edge one pixel over. */
 int qmcrt_set_math_mode(qmcrt_scene* scene, int exact);
 /* Launch shapes of the production build (math mode 0), indexes 0..count-1:
- * threads per block and warp-chunk iterations (32 rays each); shape 0 is the
- * default.  No reference counterpart: the reference launches 512-thread
- * blocks of one ray each (Util/global_function.cuh:159-197).  Any array may
- * be NULL; at most 16 shapes. */
-int qmcrt_launch_shapes(int* threads, int* chunk_iters, int* count);
+ * threads per block, warp-chunk iterations (32 rays each) and whether the
+ * launch is persistent (a grid of resident warps taking warp chunks from a
+ * work counter, instead of one warp per chunk); shape 0 is the default.  No
+ * reference counterpart: the reference launches 512-thread blocks of one
+ * ray each (Util/global_function.cuh:159-197).  Any array may be NULL; at
+ * most 16 shapes. */
+int qmcrt_launch_shapes(int* threads, int* chunk_iters, int* persistent, int* count);
 int qmcrt_set_launch_shape(qmcrt_scene* scene, int shape);
 /* Autotuner: traces heliostats[0..n) over the current light range once per
  * launch shape of the production build (after one warm-up each), keeps the

@@ -96,7 +96,7 @@ PROTOTYPES = {
     "qmcrt_batch_autotune": (_i, [_vp, _vp, _pi, _pf]),
     "qmcrt_batch_autotune_shapes": (_i, [_vp, _vp, _pi, _pf]),
     "qmcrt_batch_set_launch_shape": (_i, [_vp, _i]),
-    "qmcrt_launch_shapes": (_i, [_pi, _pi, _pi]),
+    "qmcrt_launch_shapes": (_i, [_pi, _pi, _pi, _pi]),
     "qmcrt_set_launch_shape": (_i, [_vp, _i]),
     "qmcrt_autotune": (_i, [_vp, _pi, _i, _vp, _pi, _pf]),
     "qmcrt_batch_debug_geometry": (_i, [_vp, _i, _i, _pf, _pf]),

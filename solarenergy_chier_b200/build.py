@@ -49,6 +49,8 @@ CUDA_UNITS = [
     ("tracer.cu", "tracer_fast_c128.o", ["-DQM_TRACE_VARIANT=fast_c128", "-DQM_TRACE_THREADS=32",
                                             "-DQM_TRACE_MIN_BLOCKS=28", "-DQM_CHUNK_ITERS=128", "-DQM_TRACE_FAST_DIVIDE",
                                             "-DQM_TRACE_CANDIDATE_HITS"]),
+    ("tracer.cu", "tracer_fast_ps.o", ["-DQM_TRACE_VARIANT=fast_ps", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",
+                                          "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS", "-DQM_TRACE_PERSISTENT"]),
     ("tracer.cu", "tracer_fast_t64.o", ["-DQM_TRACE_VARIANT=fast_t64", "-DQM_TRACE_THREADS=64", "-DQM_TRACE_MIN_BLOCKS=14",
                                            "-DQM_TRACE_FAST_DIVIDE", "-DQM_TRACE_CANDIDATE_HITS"]),
     ("tracer.cu", "tracer_rx.o", ["-DQM_TRACE_VARIANT=rx", "-DQM_TRACE_THREADS=32", "-DQM_TRACE_MIN_BLOCKS=28",

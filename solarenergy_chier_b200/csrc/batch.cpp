@@ -117,6 +117,7 @@ void batch_build_prefix(qmcrt_batch* b) {
   b->total_chunks = prefix.back();
   // allocated here, before any graph capture of the launch
   chunk_power_buffer(b->d_chunk_power, b->total_chunks);
+  if (b->d_work.bytes < sizeof(unsigned long long)) b->d_work.alloc(sizeof(unsigned long long));
 }
 
 cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chunk_begin, long long chunk_end) {
@@ -134,6 +135,7 @@ cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chu
   p.diag = b->d_diag.as<unsigned long long>();
   p.hit_bits = b->hit_bits;
   if (out == 0 || out == 2) p.chunk_power = b->d_chunk_power.as<double>();
+  if (out == 0) p.work_counter = b->d_work.as<unsigned long long>();
   // the prefix is laid out for the flux kernel's chunk size
   if (chunk_rays_for(b->mode, b->shape, out) != chunk_rays_for(b->mode, b->shape, 0)) return cudaErrorInvalidValue;
   return launch_trace_mode(b->mode, p, out, st, b->shape);
@@ -463,7 +465,7 @@ int qmcrt_batch_autotune_shapes(qmcrt_batch* b, void* stream, int* chosen, float
     // shape's chunk size) and the fastest kept.  Images and powers are
     // cleared afterwards.
     int n_shapes = 0;
-    qmcrt_launch_shapes(nullptr, nullptr, &n_shapes);
+    qmcrt_launch_shapes(nullptr, nullptr, nullptr, &n_shapes);
     cudaEvent_t e0, e1;
     cuda_check(cudaEventCreate(&e0), "cudaEventCreate");
     cuda_check(cudaEventCreate(&e1), "cudaEventCreate");
@@ -512,7 +514,7 @@ int qmcrt_batch_set_launch_shape(qmcrt_batch* b, int shape) {
   return guarded([&] {
     batch_checked(b);
     int n_shapes = 0;
-    qmcrt_launch_shapes(nullptr, nullptr, &n_shapes);
+    qmcrt_launch_shapes(nullptr, nullptr, nullptr, &n_shapes);
     if (shape < 0 || shape >= n_shapes) invalid("launch shape out of range");
     b->shape = shape;
     b->total_chunks = -1;

@@ -27,6 +27,7 @@ struct qmcrt_batch {
   qrt::DBuf d_bound, d_hsub, d_subv, d_verts, d_sub_free, d_sub_cand, d_sub_frames;  // per instance-grid slices
   qrt::DBuf d_images, d_power, d_diag, d_pools;
   qrt::DBuf d_chunk_power;  // per-chunk FP64 power partials of a launch (sized with the chunk prefix)
+  qrt::DBuf d_work;         // work counter of persistent flux launches
   int light_begin = 0, light_end = 0, max_lights = 0;
   long long total_chunks = -1;  // for the current light range; -1 = prefix not built
   int mode = 0;                 // 0 production, 1 exact, 2 production at 64 registers, 3 approximate math
@@ -49,7 +50,7 @@ struct qmcrt_batch {
     drop_graph();
     for (qrt::DBuf* b : {&d_grids, &d_receivers, &d_tasks, &d_prefix, &d_items, &d_rot, &d_bound, &d_hsub, &d_subv,
                     &d_verts, &d_sub_free, &d_sub_cand, &d_sub_frames, &d_images, &d_power, &d_diag, &d_pools,
-                    &d_chunk_power})
+                    &d_chunk_power, &d_work})
       b->release();
     cudaSetDevice(prev);
   }

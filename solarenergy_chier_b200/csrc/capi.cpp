@@ -432,21 +432,23 @@ qm::TraceParams base_params(qmcrt_scene* s) {
 
 // Launch shapes of the production build (math mode 0) that the autotuner
 // times: threads per block and warp-chunk iterations, all at 72 registers
-// except the 256-thread shape (64 registers, as math mode 2).  A shape
+// except the 256-thread shape (64 registers, as math mode 2), and a
+// persistent shape (resident warps taking chunks from a work counter).  A shape
 // changes how rays are handed to warps, never a ray's arithmetic.  Shapes
 // other than 0 serve flux launches only; records, hit bits and bilinear
 // deposits keep shape 0, whose chunk layout the other outputs share.
 struct LaunchShape {
-  int threads, chunk_iters;
+  int threads, chunk_iters, persistent;
   cudaError_t (*launch)(const qm::TraceParams&, int, cudaStream_t);
   int (*chunk_rays)();
 };
 const LaunchShape kShapes[] = {
-    {32, 64, qm::launch_trace_fast, qm::trace_chunk_rays_fast},
-    {32, 32, qm::launch_trace_fast_c32, qm::trace_chunk_rays_fast_c32},
-    {32, 128, qm::launch_trace_fast_c128, qm::trace_chunk_rays_fast_c128},
-    {64, 64, qm::launch_trace_fast_t64, qm::trace_chunk_rays_fast_t64},
-    {256, 64, qm::launch_trace_fast4, qm::trace_chunk_rays_fast4},
+    {32, 64, 0, qm::launch_trace_fast, qm::trace_chunk_rays_fast},
+    {32, 32, 0, qm::launch_trace_fast_c32, qm::trace_chunk_rays_fast_c32},
+    {32, 128, 0, qm::launch_trace_fast_c128, qm::trace_chunk_rays_fast_c128},
+    {64, 64, 0, qm::launch_trace_fast_t64, qm::trace_chunk_rays_fast_t64},
+    {256, 64, 0, qm::launch_trace_fast4, qm::trace_chunk_rays_fast4},
+    {32, 64, 1, qm::launch_trace_fast_ps, qm::trace_chunk_rays_fast_ps},
 };
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 
@@ -526,7 +528,11 @@ long long trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream, 
   p.total_facets = total;
   p.hit_bits = hit_bits;
   if (out == 3 && !hit_bits) return total;
-  if (out == 0) p.chunk_power = chunk_power_buffer(s->d_chunk_power, total);
+  if (out == 0) {
+    p.chunk_power = chunk_power_buffer(s->d_chunk_power, total);
+    if (s->d_work.bytes < sizeof(unsigned long long)) s->d_work.alloc(sizeof(unsigned long long));
+    p.work_counter = s->d_work.as<unsigned long long>();
+  }
   cuda_check(run_trace(s, p, out, stream), "trace kernel");
   return total;
 }
@@ -876,12 +882,13 @@ int qmcrt_trace_heliostats(qmcrt_scene* s, const int* ids, int n, void* stream) 
   return guarded([&] { trace_ids(checked(s), ids, n, static_cast<cudaStream_t>(stream)); });
 }
 
-int qmcrt_launch_shapes(int* threads, int* chunk_iters, int* count) {
+int qmcrt_launch_shapes(int* threads, int* chunk_iters, int* persistent, int* count) {
   return guarded([&] {
     if (count) *count = kNumShapes;
     for (int k = 0; k < kNumShapes; ++k) {
       if (threads) threads[k] = kShapes[k].threads;
       if (chunk_iters) chunk_iters[k] = kShapes[k].chunk_iters;
+      if (persistent) persistent[k] = kShapes[k].persistent;
     }
   });
 }

@@ -145,6 +145,7 @@ struct qmcrt_scene {
   int pool_size = 0;
   qrt::DBuf d_power, d_diag;
   qrt::DBuf d_chunk_power;  // per-chunk FP64 power partials of a launch (grows to the largest launch)
+  qrt::DBuf d_work;         // work counter of persistent flux launches
   std::vector<qm::DevTask> templates;
   qrt::DBuf d_tasks, d_prefix;
   std::vector<int> cached_ids;
@@ -187,6 +188,7 @@ struct qmcrt_scene {
     d_offset_seg.release();
     d_power.release();
     d_chunk_power.release();
+    d_work.release();
     d_diag.release();
     d_tasks.release();
     d_prefix.release();

@@ -27,6 +27,7 @@
 // evaluates the per-ray arithmetic after the shadow test with FMA
 // contraction, the hardware reciprocal square root and approximate
 // divisions (qf::); facet geometry stays explicitly rounded.
+#include <algorithm>
 #include <climits>
 
 #include "device_scene.h"
@@ -458,15 +459,16 @@ __device__ __forceinline__ void splat_bilinear(const DevReceiver& R, float X, fl
   }
 }
 
-template <int kOut>
 #ifndef QM_TRACE_MIN_BLOCKS
 #define QM_TRACE_MIN_BLOCKS 4
 #endif
-__global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
-  __shared__ FacetWindow win;
+// One warp chunk of a launch: warp = the chunk's index within the launch
+// (chunk - chunk_begin), or for per-ray records the chunk of the recorded
+// facet range.
+template <int kOut>
+__device__ __forceinline__ void trace_chunk(const TraceParams& p, FacetWindow& win, const long long warp) {
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;  // this warp's 32 window slots
-  const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int nl = p.light_end - p.light_begin;
   // Ray indexes within one heliostat fit in int: the host refuses launches
   // with num_facets * lights >= 2^31.
@@ -641,6 +643,29 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   }
 }
 
+template <int kOut>
+__global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
+  __shared__ FacetWindow win;
+  const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+#if defined(QM_TRACE_PERSISTENT)
+  // Persistent flux launches: a grid of resident warps, each taking the next
+  // warp chunk from the launch's work counter (zeroed by the launcher) until
+  // none is left.  Other outputs keep one warp per chunk.
+  if (kOut == kOutFlux && p.work_counter) {
+    const long long n = p.total_facets - p.chunk_begin;
+    for (;;) {
+      long long w = 0;
+      if ((threadIdx.x & 31) == 0) w = (long long)atomicAdd(p.work_counter, 1ull);
+      w = __shfl_sync(0xffffffffu, w, 0);
+      if (w >= n) return;
+      trace_chunk<kOut>(p, win, w);
+      __syncwarp();
+    }
+  }
+#endif
+  trace_chunk<kOut>(p, win, warp);
+}
+
 __global__ void facets_kernel(DevTask T, float3* origins, float3* normals) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= T.num_facets) return;
@@ -673,8 +698,28 @@ cudaError_t QM_SYM(launch_trace)(const TraceParams& params, int out, cudaStream_
                                  : p.total_facets - p.chunk_begin;
   if (!record && p.chunk_begin < 0) return cudaErrorInvalidValue;
   if (warps <= 0) return cudaSuccess;
-  const long long blocks = (warps + (threads / 32) - 1) / (threads / 32);
+  long long blocks = (warps + (threads / 32) - 1) / (threads / 32);
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+#if defined(QM_TRACE_PERSISTENT)
+  if (out == kOutFlux && p.work_counter) {
+    // as many blocks as stay resident together, never more than the chunks
+    static int resident = 0;
+    if (!resident) {
+      int dev = 0, sms = 0, per_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_kernel<kOutFlux>, threads, 0);
+      resident = std::max(1, sms * per_sm);
+    }
+    blocks = std::min<long long>(blocks, resident);
+    cudaError_t e = cudaMemsetAsync(p.work_counter, 0, sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return e;
+  } else {
+    p.work_counter = nullptr;
+  }
+#else
+  p.work_counter = nullptr;
+#endif
   switch (out) {
     case kOutRecord: trace_kernel<kOutRecord><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
     case kOutSplat: trace_kernel<kOutSplat><<<(unsigned)blocks, threads, 0, stream>>>(p); break;

@@ -24,6 +24,10 @@ cudaError_t launch_trace_fast_t64(const TraceParams& p, int out, cudaStream_t st
 int trace_chunk_rays_fast_c32();
 int trace_chunk_rays_fast_c128();
 int trace_chunk_rays_fast_t64();
+// Persistent launch shape: resident one-warp blocks taking warp chunks from a
+// work counter (TraceParams::work_counter) in flux launches.
+cudaError_t launch_trace_fast_ps(const TraceParams& p, int out, cudaStream_t stream);
+int trace_chunk_rays_fast_ps();
 // Production build with the arithmetic after the receiver's decisions
 // approximated (hit point, pixel position, energy).
 cudaError_t launch_trace_rx(const TraceParams& p, int out, cudaStream_t stream);

@@ -561,15 +561,17 @@ class RayTracingPipeline:
         return pipeline_run(argv)
 
 
-def launch_shapes() -> list[tuple[int, int]]:
-    """(threads per block, warp-chunk iterations) of each launch shape of the production build."""
+def launch_shapes() -> list[tuple[int, int, bool]]:
+    """(threads per block, warp-chunk iterations, persistent) of each launch shape of the production build."""
     lib = load()
     n = ctypes.c_int()
-    check(lib.qmcrt_launch_shapes(None, None, ctypes.byref(n)))
+    check(lib.qmcrt_launch_shapes(None, None, None, ctypes.byref(n)))
     t = np.zeros(n.value, np.int32)
     c = np.zeros(n.value, np.int32)
-    check(lib.qmcrt_launch_shapes(_ptr(t, ctypes.c_int), _ptr(c, ctypes.c_int), ctypes.byref(n)))
-    return list(zip(t.tolist(), c.tolist()))
+    ps = np.zeros(n.value, np.int32)
+    check(lib.qmcrt_launch_shapes(_ptr(t, ctypes.c_int), _ptr(c, ctypes.c_int), _ptr(ps, ctypes.c_int),
+                                  ctypes.byref(n)))
+    return [(a, b, bool(x)) for a, b, x in zip(t.tolist(), c.tolist(), ps.tolist())]
 
 
 def executable() -> Path:
