@@ -462,14 +462,28 @@ __device__ __forceinline__ void splat_bilinear(const DevReceiver& R, float X, fl
 #ifndef QM_TRACE_MIN_BLOCKS
 #define QM_TRACE_MIN_BLOCKS 4
 #endif
-// One warp chunk of a launch: warp = the chunk's index within the launch
-// (chunk - chunk_begin), or for per-ray records the chunk of the recorded
-// facet range.
 template <int kOut>
-__device__ __forceinline__ void trace_chunk(const TraceParams& p, FacetWindow& win, const long long warp) {
+__global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
+  __shared__ FacetWindow win;
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;  // this warp's 32 window slots
+  long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int nl = p.light_end - p.light_begin;
+#if defined(QM_TRACE_PERSISTENT)
+  // Persistent flux launches: a grid of resident warps, each taking the next
+  // warp chunk from the launch's work counter (zeroed by the launcher) until
+  // none is left; `warp` is then the chunk's index within the launch.  Other
+  // outputs keep one warp per chunk.
+  const bool persistent = kOut == kOutFlux && p.work_counter;
+  for (;;) {
+    if (persistent) {
+      long long w = 0;
+      if (lane == 0) w = (long long)atomicAdd(p.work_counter, 1ull);
+      warp = __shfl_sync(0xffffffffu, w, 0);
+      if (warp >= p.total_facets - p.chunk_begin) return;
+      __syncwarp();
+    }
+#endif
   // Ray indexes within one heliostat fit in int: the host refuses launches
   // with num_facets * lights >= 2^31.
   int t, r0, r_end;
@@ -641,29 +655,10 @@ __device__ __forceinline__ void trace_chunk(const TraceParams& p, FacetWindow& w
     if (clamped) atomicAdd(p.diag + kDiagClamped, clamped);
     if (flags & 2u) atomicAdd(p.diag + kDiagDdaCap, 1ull);
   }
-}
-
-template <int kOut>
-__global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
-  __shared__ FacetWindow win;
-  const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 #if defined(QM_TRACE_PERSISTENT)
-  // Persistent flux launches: a grid of resident warps, each taking the next
-  // warp chunk from the launch's work counter (zeroed by the launcher) until
-  // none is left.  Other outputs keep one warp per chunk.
-  if (kOut == kOutFlux && p.work_counter) {
-    const long long n = p.total_facets - p.chunk_begin;
-    for (;;) {
-      long long w = 0;
-      if ((threadIdx.x & 31) == 0) w = (long long)atomicAdd(p.work_counter, 1ull);
-      w = __shfl_sync(0xffffffffu, w, 0);
-      if (w >= n) return;
-      trace_chunk<kOut>(p, win, w);
-      __syncwarp();
-    }
+    if (!persistent) return;
   }
 #endif
-  trace_chunk<kOut>(p, win, warp);
 }
 
 __global__ void facets_kernel(DevTask T, float3* origins, float3* normals) {
