@@ -119,9 +119,6 @@ struct TraceParams {
   // order with compensation; when NULL, one double atomic per chunk
   double* chunk_power;
   unsigned long long* diag;
-  // flux launches of the persistent launch shape: the launch's work counter
-  // (next warp chunk to take; zeroed by the launcher), else NULL
-  unsigned long long* work_counter;
   // bilinear-deposit and hit-bit variants: one word per warp iteration of the
   // launch (chunk - chunk_begin), bit i = lane i's ray hit the receiver; may
   // be NULL for the bilinear deposit
@@ -130,6 +127,9 @@ struct TraceParams {
   int32_t* records;
   int record_task;
   int record_facet_begin, record_facet_end;
+  // flux launches of the persistent launch shape: the launch's work counter
+  // (next warp chunk to take; zeroed by the launcher), else NULL
+  unsigned long long* work_counter;
 };
 
 }  // namespace qm

@@ -459,15 +459,19 @@ __device__ __forceinline__ void splat_bilinear(const DevReceiver& R, float X, fl
   }
 }
 
+template <int kOut>
 #ifndef QM_TRACE_MIN_BLOCKS
 #define QM_TRACE_MIN_BLOCKS 4
 #endif
-template <int kOut>
 __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
   __shared__ FacetWindow win;
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;  // this warp's 32 window slots
+#if defined(QM_TRACE_PERSISTENT)
   long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+#else
+  const long long warp = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+#endif
   const int nl = p.light_end - p.light_begin;
 #if defined(QM_TRACE_PERSISTENT)
   // Persistent flux launches: a grid of resident warps, each taking the next
