@@ -135,10 +135,9 @@ cudaError_t batch_launch(qmcrt_batch* b, cudaStream_t st, int out, long long chu
   p.diag = b->d_diag.as<unsigned long long>();
   p.hit_bits = b->hit_bits;
   if (out == 0 || out == 2) p.chunk_power = b->d_chunk_power.as<double>();
-  if (out == 0) p.work_counter = b->d_work.as<unsigned long long>();
   // the prefix is laid out for the flux kernel's chunk size
   if (chunk_rays_for(b->mode, b->shape, out) != chunk_rays_for(b->mode, b->shape, 0)) return cudaErrorInvalidValue;
-  return launch_trace_mode(b->mode, p, out, st, b->shape);
+  return launch_trace_mode(b->mode, p, out, st, b->shape, out == 0 ? b->d_work.as<unsigned long long>() : nullptr);
 }
 
 }  // namespace qrt

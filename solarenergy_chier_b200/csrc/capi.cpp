@@ -439,7 +439,7 @@ qm::TraceParams base_params(qmcrt_scene* s) {
 // deposits keep shape 0, whose chunk layout the other outputs share.
 struct LaunchShape {
   int threads, chunk_iters, persistent;
-  cudaError_t (*launch)(const qm::TraceParams&, int, cudaStream_t);
+  cudaError_t (*launch)(const qm::TraceParams&, int, cudaStream_t, unsigned long long*);
   int (*chunk_rays)();
 };
 const LaunchShape kShapes[] = {
@@ -458,14 +458,15 @@ long long chunk_rays_for(int mode, int shape, int out) {
   return kShapes[shape_for(mode, shape, out)].chunk_rays();
 }
 
-cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st, int shape) {
+cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st, int shape,
+                              unsigned long long* work_counter) {
   cudaError_t e;
   switch (mode) {
     case 1: e = qm::launch_trace_exact(p, out, st); break;
     case 2: e = qm::launch_trace_fast4(p, out, st); break;
     case 3: e = qm::launch_trace_approx(p, out, st); break;
     case 4: e = qm::launch_trace_rx(p, out, st); break;
-    default: e = kShapes[shape_for(mode, shape, out)].launch(p, out, st); break;
+    default: e = kShapes[shape_for(mode, shape, out)].launch(p, out, st, work_counter); break;
   }
   // flux and bilinear-deposit launches add their per-chunk power partials
   if (e == cudaSuccess && (out == 0 || out == 2) && p.chunk_power) e = qm::launch_power_reduce(p, st);
@@ -478,8 +479,9 @@ double* chunk_power_buffer(DBuf& buf, long long chunks) {
   return buf.as<double>();
 }
 
-cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st) {
-  return launch_trace_mode(s->exact, p, out, st, s->shape);
+cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st,
+                      unsigned long long* work_counter) {
+  return launch_trace_mode(s->exact, p, out, st, s->shape, work_counter);
 }
 
 // Traces heliostats ids[0..n) over the scene's light range: out 0 adds their
@@ -528,12 +530,13 @@ long long trace_ids(qmcrt_scene* s, const int* ids, int n, cudaStream_t stream, 
   p.total_facets = total;
   p.hit_bits = hit_bits;
   if (out == 3 && !hit_bits) return total;
+  unsigned long long* work = nullptr;
   if (out == 0) {
     p.chunk_power = chunk_power_buffer(s->d_chunk_power, total);
     if (s->d_work.bytes < sizeof(unsigned long long)) s->d_work.alloc(sizeof(unsigned long long));
-    p.work_counter = s->d_work.as<unsigned long long>();
+    work = s->d_work.as<unsigned long long>();
   }
-  cuda_check(run_trace(s, p, out, stream), "trace kernel");
+  cuda_check(run_trace(s, p, out, stream, work), "trace kernel");
   return total;
 }
 

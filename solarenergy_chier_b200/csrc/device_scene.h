@@ -127,9 +127,6 @@ struct TraceParams {
   int32_t* records;
   int record_task;
   int record_facet_begin, record_facet_end;
-  // flux launches of the persistent launch shape: the launch's work counter
-  // (next warp chunk to take; zeroed by the launcher), else NULL
-  unsigned long long* work_counter;
 };
 
 }  // namespace qm

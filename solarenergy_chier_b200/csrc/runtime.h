@@ -207,13 +207,16 @@ qmcrt_scene* checked(qmcrt_scene* s);
 // shadow-free test (tan_local < 0: unbounded, tan_world < 0).
 void sun_cone(float3 sun_dir, float tan_local, float3& axis, float& tan_world);
 // out: 0 flux, 1 per-ray outcome codes, 2 bilinear deposit, 3 hit bits
-// (qm::TraceOut in tracer.cu); mode: the kernel build (qmcrt_set_math_mode).
-cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st, int shape = 0);
+// (qm::TraceOut in tracer.cu); mode: the kernel build (qmcrt_set_math_mode);
+// work_counter: one device word, used by flux launches of the persistent shape.
+cudaError_t launch_trace_mode(int mode, const qm::TraceParams& p, int out, cudaStream_t st, int shape = 0,
+                              unsigned long long* work_counter = nullptr);
 // Rays per warp chunk of the kernel a launch of (mode, shape, out) runs.
 long long chunk_rays_for(int mode, int shape, int out);
 // Grow-only buffer of per-chunk power partials for a launch of `chunks` warp chunks.
 double* chunk_power_buffer(DBuf& buf, long long chunks);
-cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st);
+cudaError_t run_trace(const qmcrt_scene* s, const qm::TraceParams& p, int out, cudaStream_t st,
+                      unsigned long long* work_counter = nullptr);
 int trace_chunk_rays();
 constexpr long long kMaxTaskRays = 0x7fffffffLL - 0x10000;
 

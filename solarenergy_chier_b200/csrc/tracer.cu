@@ -459,11 +459,19 @@ __device__ __forceinline__ void splat_bilinear(const DevReceiver& R, float X, fl
   }
 }
 
+// The persistent build's kernels take the launch's work counter as a second
+// argument; the other builds keep TraceParams as their only argument.
+#if defined(QM_TRACE_PERSISTENT)
+#define QM_TRACE_ARGS TraceParams p, unsigned long long* work_counter
+#else
+#define QM_TRACE_ARGS TraceParams p
+#endif
+
 template <int kOut>
 #ifndef QM_TRACE_MIN_BLOCKS
 #define QM_TRACE_MIN_BLOCKS 4
 #endif
-__global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(TraceParams p) {
+__global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(QM_TRACE_ARGS) {
   __shared__ FacetWindow win;
   const int lane = threadIdx.x & 31;
   const int wbase = threadIdx.x & ~31;  // this warp's 32 window slots
@@ -478,11 +486,11 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(Tr
   // warp chunk from the launch's work counter (zeroed by the launcher) until
   // none is left; `warp` is then the chunk's index within the launch.  Other
   // outputs keep one warp per chunk.
-  const bool persistent = kOut == kOutFlux && p.work_counter;
+  const bool persistent = kOut == kOutFlux && work_counter;
   for (;;) {
     if (persistent) {
       long long w = 0;
-      if (lane == 0) w = (long long)atomicAdd(p.work_counter, 1ull);
+      if (lane == 0) w = (long long)atomicAdd(work_counter, 1ull);
       warp = __shfl_sync(0xffffffffu, w, 0);
       if (warp >= p.total_facets - p.chunk_begin) return;
       __syncwarp();
@@ -685,7 +693,8 @@ cudaError_t QM_SYM(launch_facets)(const DevTask& task, float3* origins, float3* 
 
 int QM_SYM(trace_chunk_rays)() { return kChunk; }
 
-cudaError_t QM_SYM(launch_trace)(const TraceParams& params, int out, cudaStream_t stream) {
+cudaError_t QM_SYM(launch_trace)(const TraceParams& params, int out, cudaStream_t stream,
+                                 unsigned long long* work_counter) {
   const int threads = kThreads;
   const long long nl = params.light_end - params.light_begin;
   if (nl <= 0) return cudaSuccess;
@@ -700,7 +709,7 @@ cudaError_t QM_SYM(launch_trace)(const TraceParams& params, int out, cudaStream_
   long long blocks = (warps + (threads / 32) - 1) / (threads / 32);
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
 #if defined(QM_TRACE_PERSISTENT)
-  if (out == kOutFlux && p.work_counter) {
+  if (out == kOutFlux && work_counter) {
     // as many blocks as stay resident together, never more than the chunks
     static int resident = 0;
     if (!resident) {
@@ -711,19 +720,21 @@ cudaError_t QM_SYM(launch_trace)(const TraceParams& params, int out, cudaStream_
       resident = std::max(1, sms * per_sm);
     }
     blocks = std::min<long long>(blocks, resident);
-    cudaError_t e = cudaMemsetAsync(p.work_counter, 0, sizeof(unsigned long long), stream);
+    cudaError_t e = cudaMemsetAsync(work_counter, 0, sizeof(unsigned long long), stream);
     if (e != cudaSuccess) return e;
   } else {
-    p.work_counter = nullptr;
+    work_counter = nullptr;
   }
+#define QM_TRACE_LAUNCH_ARGS p, work_counter
 #else
-  p.work_counter = nullptr;
+  (void)work_counter;
+#define QM_TRACE_LAUNCH_ARGS p
 #endif
   switch (out) {
-    case kOutRecord: trace_kernel<kOutRecord><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
-    case kOutSplat: trace_kernel<kOutSplat><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
-    case kOutBits: trace_kernel<kOutBits><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
-    default: trace_kernel<kOutFlux><<<(unsigned)blocks, threads, 0, stream>>>(p); break;
+    case kOutRecord: trace_kernel<kOutRecord><<<(unsigned)blocks, threads, 0, stream>>>(QM_TRACE_LAUNCH_ARGS); break;
+    case kOutSplat: trace_kernel<kOutSplat><<<(unsigned)blocks, threads, 0, stream>>>(QM_TRACE_LAUNCH_ARGS); break;
+    case kOutBits: trace_kernel<kOutBits><<<(unsigned)blocks, threads, 0, stream>>>(QM_TRACE_LAUNCH_ARGS); break;
+    default: trace_kernel<kOutFlux><<<(unsigned)blocks, threads, 0, stream>>>(QM_TRACE_LAUNCH_ARGS); break;
   }
   return cudaGetLastError();
 }
