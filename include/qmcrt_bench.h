@@ -24,6 +24,12 @@ int qmcrt_microbench_atomics(int n_pixels, double* giga_per_s);
 int qmcrt_microbench_atomics_replay(const int* device_codes, long long n_codes, int n_pixels, int repeats,
                                     double* ms_per_launch);
 
+/* Checks the tracer's own correctly rounded float primitives against CUDA's
+ * on every 32-bit input pattern: mismatches[0] = inputs where the device
+ * qm_rn_rsqrt (series refinement of the hardware estimate) differs from
+ * __frsqrt_rn.  Entries past the primitives checked are set to 0. */
+int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count);
+
 #ifdef __cplusplus
 }
 #endif

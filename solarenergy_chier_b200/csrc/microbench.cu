@@ -4,8 +4,20 @@
 #include <stdint.h>
 
 #include "qmcrt_bench.h"
+#include "vecmath.h"
 
 namespace {
+
+// Own correctly rounded primitives against CUDA's, one float bit pattern per
+// thread (bits = begin + thread index): counts[0] = patterns where
+// qm_rn_rsqrt differs from __frsqrt_rn (bit for bit; NaN results compare as
+// NaN).
+__global__ void primitives_kernel(unsigned begin, unsigned long long* counts) {
+  const unsigned bits = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  const float x = __uint_as_float(bits);
+  const float a = qm_rn_rsqrt(x), b = __frsqrt_rn(x);
+  if (__float_as_uint(a) != __float_as_uint(b) && !(a != a && b != b)) atomicAdd(counts + 0, 1ull);
+}
 
 __global__ void fma_kernel(float* out, int iters, float a, float b) {
   float x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
@@ -105,6 +117,22 @@ extern "C" int qmcrt_microbench_atomics_replay(const int* device_codes, long lon
   cudaFree(c.img);
   if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return 3;
   *ms_per_launch = (double)ms;
+  return 0;
+}
+
+extern "C" int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count) {
+  if (!mismatches || count < 1) return 1;
+  unsigned long long* d = nullptr;
+  if (cudaMalloc(&d, sizeof(unsigned long long) * 1) != cudaSuccess) return 3;
+  cudaMemset(d, 0, sizeof(unsigned long long) * 1);
+  // every 32-bit pattern: 16 launches of 2^28 threads
+  for (unsigned long long begin = 0; begin < (1ull << 32); begin += (1ull << 28))
+    primitives_kernel<<<(1u << 28) / 256, 256>>>((unsigned)begin, d);
+  unsigned long long h[1] = {0};
+  const cudaError_t e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return 3;
+  for (int k = 0; k < count; ++k) mismatches[k] = k < 1 ? h[k] : 0;
   return 0;
 }
 

@@ -36,3 +36,15 @@ def l2_atomics_replay_per_s(device_codes_ptr: int, n_codes: int, n_hits: int, n_
     ms = ctypes.c_double()
     check(fn(ctypes.c_void_p(device_codes_ptr), int(n_codes), int(n_pixels), int(repeats), ctypes.byref(ms)))
     return n_hits * repeats / (ms.value * 1e-3)
+
+
+def primitive_mismatches(count: int = 1) -> list[int]:
+    """Inputs (of all 2^32 float bit patterns) where the tracer's own
+    correctly rounded primitives differ from CUDA's: [rsqrt]."""
+    lib = load()
+    fn = lib.qmcrt_debug_check_primitives
+    fn.restype = ctypes.c_int
+    fn.argtypes = [ctypes.POINTER(ctypes.c_ulonglong), ctypes.c_int]
+    out = (ctypes.c_ulonglong * count)()
+    check(fn(out, count))
+    return [int(v) for v in out]

@@ -84,6 +84,7 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
     prod_vs_fp64 = host_vs_fp64 = 0
     approx_dec = approx_same = approx_vs_fp64 = 0
     exact_shift = 0
+    pixel_moves = 0
     rx_dec = rx_same = 0
     W = s.receiver(0)["width"]
     for h in ids:
@@ -116,6 +117,18 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
         s.set_math_mode(0)
         got = s.hit_records(h, fb, fe, 0, L)
         n += got.size
+        # production vs exact build where both hit: the pixel may move by one
+        # row or column (the production build takes the cylinder's v from the
+        # device acosf times a rounded 1/(2 pi), the exact build from a double
+        # arc cosine divided by 2 pi), never further
+        both = (got >= 0) & (exact >= 0) & (got != exact)
+        if np.any(both):
+            a, b = got[both], exact[both]
+            drow = np.abs(a // W - b // W)
+            dcol = np.abs(a % W - b % W)
+            dcol = np.minimum(dcol, W - dcol)
+            assert np.all(drow + dcol == 1), f"heliostat {h}: production pixel more than one step from the exact build's"
+            pixel_moves += int(both.sum())
         prod_dec += int(np.count_nonzero((got >= 0) == (want >= 0)))
         prod_same += int(np.count_nonzero(got == want))
         prod_vs_fp64 += int(np.count_nonzero((got >= 0) != (ref64 >= 0)))
@@ -123,11 +136,13 @@ def test_per_ray_outcomes_on_the_benchmark_field(field):
     print("per-ray on the benchmark field:", json.dumps(
         {"rays": n, "decision_agreement": prod_dec / n, "outcome_agreement": prod_same / n,
          "exact_build_column_shifts": exact_shift / n,
+         "production_pixel_moves_vs_exact_build": pixel_moves / n,
          "approx_math": {"decision_agreement": approx_dec / n, "outcome_agreement": approx_same / n},
          "approx_receiver": {"decision_agreement": rx_dec / n, "outcome_agreement": rx_same / n},
          "decision_flips_vs_fp64": {"production": prod_vs_fp64 / n, "host_arithmetic": host_vs_fp64 / n,
                                     "approx_math": approx_vs_fp64 / n}}))
     assert exact_shift <= 3e-6 * n
+    assert pixel_moves <= 1e-3 * n
     assert prod_dec >= 0.9999 * n
     assert prod_same >= 0.999 * n
     assert approx_vs_fp64 <= host_vs_fp64 + 1e-5 * n
