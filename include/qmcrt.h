@@ -118,7 +118,11 @@ int qmcrt_heliostat_facets(qmcrt_scene* scene, int heliostat, float* origins, fl
  * Injection point for parity runs (the pool replacement of
  * Tests/QuasiMonteCarloRayTracingTests/receiverIntersectUtil.cpp:8-33):
  * dirs_xyz and perturb_xyz hold groups*per_group float3 each, host memory
- * (on_device = 0) or device memory (on_device = 1). */
+ * (on_device = 0) or device memory (on_device = 1).  Every vector must be a
+ * unit vector: one whose squared length lies outside [0.25, 4] (or is NaN)
+ * is refused with QMCRT_ERR_INVALID and the scene keeps its pools (the
+ * reference's pools are unit vectors by construction; the tracer normalises
+ * the perturbed normal and the reflected ray without a range test). */
 int qmcrt_set_sample_pool(qmcrt_scene* scene, const float* dirs_xyz, const float* perturb_xyz, int groups,
                           int per_group, int on_device);
 /* Regenerates both pools on the device (replaces SceneProcessor::set_samplelights

@@ -27,7 +27,9 @@ int qmcrt_microbench_atomics_replay(const int* device_codes, long long n_codes, 
 /* Checks the tracer's own correctly rounded float primitives against CUDA's
  * on every 32-bit input pattern: mismatches[0] = inputs where the device
  * qm_rn_rsqrt (series refinement of the hardware estimate) differs from
- * __frsqrt_rn.  Entries past the primitives checked are set to 0. */
+ * __frsqrt_rn, mismatches[1] = inputs in [2^-125, 2^125) where the series
+ * without its range test (qm_rn_rsqrt_unit) does.  Entries past the
+ * primitives checked are set to 0. */
 int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count);
 
 #ifdef __cplusplus

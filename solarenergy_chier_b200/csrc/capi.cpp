@@ -778,14 +778,26 @@ int qmcrt_set_sample_pool(qmcrt_scene* s, const float* dirs, const float* pertur
       invalid("pool shape must match the configuration's groups x lights-per-group");
     DeviceGuard guard(s->device);
     const int n = s->pool_size;
-    // staging for both xyz pools, kept with the scene (allocated once)
+    // staging for both xyz pools and a counter word after them, kept with the
+    // scene (allocated once)
     DBuf& tmp = s->d_pool_stage;
-    tmp.alloc((size_t)n * 6 * sizeof(float));
+    const size_t stage_bytes = (size_t)n * 6 * sizeof(float) + sizeof(unsigned);
+    if (tmp.bytes < stage_bytes) tmp.alloc(stage_bytes);
     float* stage_dirs = tmp.as<float>();
     float* stage_pert = stage_dirs + (size_t)n * 3;
+    unsigned* bad = reinterpret_cast<unsigned*>(stage_pert + (size_t)n * 3);
     const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     cuda_check(cudaMemcpy(stage_dirs, dirs, (size_t)n * 3 * sizeof(float), kind), "pool upload");
     cuda_check(cudaMemcpy(stage_pert, perturb, (size_t)n * 3 * sizeof(float), kind), "pool upload");
+    // Both pools must hold unit vectors (the tracer normalises the perturbed
+    // normal and the reflected ray without a range test); the scene's pools
+    // are left as they were when a vector is refused.
+    cuda_check(cudaMemsetAsync(bad, 0, sizeof(unsigned), 0), "pool check");
+    cuda_check(qm::launch_count_non_unit(stage_dirs, n, bad, 0), "pool check");
+    cuda_check(qm::launch_count_non_unit(stage_pert, n, bad, 0), "pool check");
+    unsigned h_bad = 0;
+    cuda_check(cudaMemcpy(&h_bad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost), "pool check");
+    if (h_bad) invalid("sample-pool vectors must be unit vectors (squared length in [0.25, 4])");
     cuda_check(qm::launch_xyz_to_float4(stage_dirs, s->d_samples.as<float4>(), n, 0), "pool convert");
     cuda_check(qm::launch_xyz_to_float4(stage_pert, s->d_perturb.as<float4>(), n, 0), "pool convert");
     cuda_check(cudaDeviceSynchronize(), "pool convert");

@@ -11,12 +11,15 @@ namespace {
 // Own correctly rounded primitives against CUDA's, one float bit pattern per
 // thread (bits = begin + thread index): counts[0] = patterns where
 // qm_rn_rsqrt differs from __frsqrt_rn (bit for bit; NaN results compare as
-// NaN).
+// NaN), counts[1] = patterns in [2^-125, 2^125) where qm_rn_rsqrt_unit (no
+// range test) does.
 __global__ void primitives_kernel(unsigned begin, unsigned long long* counts) {
   const unsigned bits = begin + blockIdx.x * blockDim.x + threadIdx.x;
   const float x = __uint_as_float(bits);
   const float a = qm_rn_rsqrt(x), b = __frsqrt_rn(x);
   if (__float_as_uint(a) != __float_as_uint(b) && !(a != a && b != b)) atomicAdd(counts + 0, 1ull);
+  if (x >= 0x1p-125f && x < 0x1p125f && __float_as_uint(qm_rn_rsqrt_unit(x)) != __float_as_uint(b))
+    atomicAdd(counts + 1, 1ull);
 }
 
 __global__ void fma_kernel(float* out, int iters, float a, float b) {
@@ -121,18 +124,19 @@ extern "C" int qmcrt_microbench_atomics_replay(const int* device_codes, long lon
 }
 
 extern "C" int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count) {
+  constexpr int kChecks = 2;
   if (!mismatches || count < 1) return 1;
   unsigned long long* d = nullptr;
-  if (cudaMalloc(&d, sizeof(unsigned long long) * 1) != cudaSuccess) return 3;
-  cudaMemset(d, 0, sizeof(unsigned long long) * 1);
+  if (cudaMalloc(&d, sizeof(unsigned long long) * kChecks) != cudaSuccess) return 3;
+  cudaMemset(d, 0, sizeof(unsigned long long) * kChecks);
   // every 32-bit pattern: 16 launches of 2^28 threads
   for (unsigned long long begin = 0; begin < (1ull << 32); begin += (1ull << 28))
     primitives_kernel<<<(1u << 28) / 256, 256>>>((unsigned)begin, d);
-  unsigned long long h[1] = {0};
+  unsigned long long h[kChecks] = {0, 0};
   const cudaError_t e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return 3;
-  for (int k = 0; k < count; ++k) mismatches[k] = k < 1 ? h[k] : 0;
+  for (int k = 0; k < count; ++k) mismatches[k] = k < kChecks ? h[k] : 0;
   return 0;
 }
 

@@ -132,6 +132,20 @@ __global__ void pool_tan_kernel(const float4* pool, int n, unsigned* out) {
   if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(t));
 }
 
+// Counts the xyz vectors whose squared length lies outside [0.25, 4] or is
+// NaN (one warp-aggregated atomic per warp).
+__global__ void count_non_unit_kernel(const float* xyz, int n, unsigned* bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool b = false;
+  if (i < n) {
+    const float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+    const float s = x * x + y * y + z * z;
+    b = !(s >= 0.25f && s <= 4.0f);
+  }
+  const unsigned votes = __ballot_sync(0xffffffffu, b);
+  if ((threadIdx.x & 31) == 0 && votes) atomicAdd(bad, (unsigned)__popc(votes));
+}
+
 __global__ void xyz_to_float4_kernel(const float* xyz, float4* out, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -169,6 +183,12 @@ cudaError_t launch_trace_pools(const float4* samples, const float4* perturbation
 cudaError_t launch_pool_tan(const float4* pool, int n, unsigned* out, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   pool_tan_kernel<<<(n + 255) / 256, 256, 0, stream>>>(pool, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_non_unit(const float* xyz, int n, unsigned* bad, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  count_non_unit_kernel<<<(n + 255) / 256, 256, 0, stream>>>(xyz, n, bad);
   return cudaGetLastError();
 }
 

@@ -45,6 +45,9 @@ struct PoolParams {
 cudaError_t launch_pool(const PoolParams& p, cudaStream_t stream);
 cudaError_t launch_offsets(int* out, long long count, uint32_t seed, int heliostat, int pool, cudaStream_t stream);
 cudaError_t launch_xyz_to_float4(const float* xyz, float4* out, int n, cudaStream_t stream);
+// Adds to *bad the number of the n xyz vectors whose squared length is outside
+// [0.25, 4] or NaN.
+cudaError_t launch_count_non_unit(const float* xyz, int n, unsigned* bad, cudaStream_t stream);
 // *out (zeroed by the caller) = bits of the largest tan(angle from +y) over
 // the pool (+inf if some direction has y <= 0).
 cudaError_t launch_pool_tan(const float4* pool, int n, unsigned* out, cudaStream_t stream);

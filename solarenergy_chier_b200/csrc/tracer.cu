@@ -599,8 +599,14 @@ __global__ void __launch_bounds__(kThreads, QM_TRACE_MIN_BLOCKS) trace_kernel(QM
         nframe.identity = (__float_as_int(wn.w) & 1) != 0;
         const int g1 = __float_as_int(lds(win.u[slot]).w);
         const int b = (g1 & 0x7fffffff) + lab;
-        float3 n = qx::normalize(qx::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
-        float3 rd = qx::normalize(qx::reflect(neg(dir), n));
+        // Both normalisations take vectors of unit scale: the pools hold unit
+        // vectors (qmcrt_set_sample_pool refuses squared lengths outside
+        // [0.25, 4]), the facet frames are orthonormal (or NaN), and the
+        // reflection keeps the direction's length, so the squared lengths lie
+        // far inside the series' range [2^-125, 2^125) and normalize_unit
+        // drops the range test.
+        float3 n = qx::normalize_unit(qx::to_world(nframe, xyz(__ldg(lds_ptr(win.perturbations[threadIdx.x >> 5]) + b))));
+        float3 rd = qx::normalize_unit(qx::reflect(neg(dir), n));
         // Facets of sub-heliostats no other heliostat can block skip the
         // block walk; where only a few listed heliostats can
         // (qm::block_candidates, decided per sun with the pools),

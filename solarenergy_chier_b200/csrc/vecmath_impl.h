@@ -4,7 +4,7 @@
 // divide rounds separately, as in the CPU oracle, whatever the compilation
 // flags), and with plain operators plus the approximate reciprocal square
 // root and division (namespace qf, the approximate-math tracer build).  QR
-// is the reciprocal square root.  No include guard on purpose.
+// is the reciprocal square root, QRU the same for arguments of unit scale.  No include guard on purpose.
 
 
 
@@ -25,6 +25,9 @@ QM_HD float3 cross(float3 a, float3 b) {
 QM_HD float rlen(float d) { return QR(d); }
 QM_HD float length(float3 v) { return sqrtf(dot(v, v)); }
 QM_HD float3 normalize(float3 v) { float inv = rlen(dot(v, v)); return mul(v, inv); }
+// normalize for vectors of unit scale (squared length in [2^-125, 2^125) or
+// NaN): the same value without the reciprocal square root's range test (QRU).
+QM_HD float3 normalize_unit(float3 v) { float inv = QRU(dot(v, v)); return mul(v, inv); }
 QM_HD float3 reflect(float3 i, float3 n) { return sub(i, mul(mul(n, 2.0f), dot(n, i))); }
 
 QM_HD float dot2(float2 a, float2 b) { return QA(QM(a.x, b.x), QM(a.y, b.y)); }

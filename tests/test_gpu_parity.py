@@ -179,6 +179,20 @@ def test_errors_are_reported_not_raised_on_device(small):
         s.set_light_range(0, s.lights_per_group + 1)
     with pytest.raises(q.QmcrtError):
         s.set_sample_pool(small.dirs[:-1], small.pert[:-1])
+    # pools of non-unit vectors are refused and the scene keeps its pools
+    before = s.get_sample_pool()
+    for bad in (0.0, 0.49, 2.01, np.nan):
+        d = small.dirs.copy()
+        d[7] = d[7] * bad
+        with pytest.raises(q.QmcrtError) as e:
+            s.set_sample_pool(d, small.pert)
+        assert e.value.code == 1 and "unit" in str(e.value)
+        p = small.pert.copy()
+        p[-1] = p[-1] * bad
+        with pytest.raises(q.QmcrtError):
+            s.set_sample_pool(small.dirs, p)
+    after = s.get_sample_pool()
+    assert all(np.array_equal(a, b) for a, b in zip(before, after))
     s.trace([])  # empty list is a no-op
 
 
