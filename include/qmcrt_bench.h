@@ -28,8 +28,12 @@ int qmcrt_microbench_atomics_replay(const int* device_codes, long long n_codes, 
  * on every 32-bit input pattern: mismatches[0] = inputs where the device
  * qm_rn_rsqrt (series refinement of the hardware estimate) differs from
  * __frsqrt_rn, mismatches[1] = inputs in [2^-125, 2^125) where the series
- * without its range test (qm_rn_rsqrt_unit) does.  Entries past the
- * primitives checked are set to 0. */
+ * without its range test (qm_rn_rsqrt_unit) does; over 12 receiver heights h
+ * from 1 mm to 1 km and every pattern a, mismatches[2] = quotients
+ * qm_div_by_rcp(a, h, RN(1/h)) that differ from __fdiv_rn(a, h) with a and
+ * the quotient in [2^-90, 2^90],
+ * mismatches[3] = u = quotient + 0.5 that differ while either lies in [0, 1].
+ * Entries past the checks are set to 0. */
 int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count);
 
 #ifdef __cplusplus

@@ -208,6 +208,9 @@ void build_device_scene(qmcrt_scene* s) {
     }
     dr.pos = r.pos;
     dr.size = r.size;
+    // the loader refuses empty images, so the height lies in [1/ppm, 2^31/ppm]
+    // and its reciprocal is a normal float
+    dr.rcp_height = r.type == 1 ? 1.0f / r.size.y : 0.0f;
     s->receivers.push_back(dr);
     s->images.push_back(std::move(img));
   }

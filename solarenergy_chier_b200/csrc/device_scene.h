@@ -44,6 +44,7 @@ struct DevReceiver {
   double* deposit;      // bilinear-deposit launches: FP64 accumulator of the same shape (else unused)
   float3 a, ab, ac;     // rectangle: vertex 0, v1 - v0, v3 - v0
   float3 pos, size;     // cylinder: centre, (radius, height, -)
+  float rcp_height;     // cylinder: 1 / height rounded to nearest (host division)
 };
 
 // One heliostat to trace (a HeliostatArgument plus the per-heliostat

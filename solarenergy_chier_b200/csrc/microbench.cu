@@ -22,6 +22,25 @@ __global__ void primitives_kernel(unsigned begin, unsigned long long* counts) {
     atomicAdd(counts + 1, 1ull);
 }
 
+// Division by a height h with the precomputed y = RN(1/h) (the cylinder's u):
+// counts[2] = patterns a where the quotient differs from __fdiv_rn(a, h) while
+// a and the quotient lie in [2^-90, 2^90] (Markstein's theorem needs the
+// remainder a - h q, about 2^-24 a, to stay normal), counts[3] = patterns
+// where u = q + 0.5 differs while either u lies in [0, 1] (where it decides a
+// hit and a pixel row): none, since below that range u rounds to 0.5 either
+// way.
+__global__ void division_kernel(unsigned begin, float h, float y, unsigned long long* counts) {
+  const unsigned bits = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  const float a = __uint_as_float(bits);
+  const float q = qm_div_by_rcp(a, h, y), w = __fdiv_rn(a, h);
+  const float aw = fabsf(w), aa = fabsf(a);
+  if (aw >= 0x1p-90f && aw <= 0x1p90f && aa >= 0x1p-90f && aa <= 0x1p90f && __float_as_uint(q) != __float_as_uint(w))
+    atomicAdd(counts + 2, 1ull);
+  const float u = __fadd_rn(q, 0.5f), uw = __fadd_rn(w, 0.5f);
+  const bool in = (u >= 0.0f && u <= 1.0f) || (uw >= 0.0f && uw <= 1.0f);
+  if (in && __float_as_uint(u) != __float_as_uint(uw)) atomicAdd(counts + 3, 1ull);
+}
+
 __global__ void fma_kernel(float* out, int iters, float a, float b) {
   float x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
   for (int i = 0; i < iters; ++i) {
@@ -124,7 +143,7 @@ extern "C" int qmcrt_microbench_atomics_replay(const int* device_codes, long lon
 }
 
 extern "C" int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count) {
-  constexpr int kChecks = 2;
+  constexpr int kChecks = 4;
   if (!mismatches || count < 1) return 1;
   unsigned long long* d = nullptr;
   if (cudaMalloc(&d, sizeof(unsigned long long) * kChecks) != cudaSuccess) return 3;
@@ -132,11 +151,16 @@ extern "C" int qmcrt_debug_check_primitives(unsigned long long* mismatches, int 
   // every 32-bit pattern: 16 launches of 2^28 threads
   for (unsigned long long begin = 0; begin < (1ull << 32); begin += (1ull << 28))
     primitives_kernel<<<(1u << 28) / 256, 256>>>((unsigned)begin, d);
-  unsigned long long h[kChecks] = {0, 0};
-  const cudaError_t e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+  // receiver heights from a millimetre to a kilometre
+  const float heights[] = {12.0f, 4.0f, 7.3f, 0.37f, 123.4f, 0.003f, 1000.0f, 1.0f, 3.0f, 0.1f, 6.0f, 17.77f};
+  for (float h : heights)
+    for (unsigned long long begin = 0; begin < (1ull << 32); begin += (1ull << 28))
+      division_kernel<<<(1u << 28) / 256, 256>>>((unsigned)begin, h, 1.0f / h, d);
+  unsigned long long host[kChecks] = {0, 0, 0, 0};
+  const cudaError_t e = cudaMemcpy(host, d, sizeof host, cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return 3;
-  for (int k = 0; k < count; ++k) mismatches[k] = k < kChecks ? h[k] : 0;
+  for (int k = 0; k < count; ++k) mismatches[k] = k < kChecks ? host[k] : 0;
   return 0;
 }
 

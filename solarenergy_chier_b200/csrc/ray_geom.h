@@ -32,7 +32,11 @@ __device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, flo
   float t_plus = delta <= 0.0f ? r.size.x : sqrtf(qm_rn_sub(r2, delta));
   t = qm_rn_div(qm_rn_sub(tp, t_plus), qs::length2(make_float2(d.x, d.z)));
   float3 ip = qs::add(qs::mul(d, t), o);
-  u = qm_rn_add(qm_rn_div(qm_rn_sub(ip.y, r.pos.y), r.size.y), 0.5f);
+  // (ip.y - pos.y) / height by Markstein's division with the host's RN(1/height):
+  // equal to the correctly rounded quotient wherever it and the numerator lie
+  // in [2^-90, 2^90]; below that u rounds to 0.5 either way, and where the
+  // product overflows u is infinite (a miss) either way.
+  u = qm_rn_add(qm_div_by_rcp(qm_rn_sub(ip.y, r.pos.y), r.size.y, r.rcp_height), 0.5f);
   if (u < 0.0f || u > 1.0f) return false;
   float2 cs = qs::normalize2(make_float2(qm_rn_sub(ip.x, r.pos.x), qm_rn_sub(ip.z, r.pos.z)));
   float cx = fminf(fmaxf(cs.x, -1.0f), 1.0f);

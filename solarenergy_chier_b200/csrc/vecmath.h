@@ -118,6 +118,28 @@ QM_HD float qm_rn_rsqrt_unit(float x) {
   return (float)(1.0 / sqrt((double)x));
 #endif
 }
+// a / b rounded to nearest, given y = RN(1/b) (b and y normal): Markstein's
+// division -- q = RN(a y) lies within one ulp of a/b, so r = a - b q is
+// exact (one FMA) and RN(q + r y) = RN(a/b) (Muller et al., Handbook of
+// Floating-Point Arithmetic, Markstein's theorem) -- wherever the remainder
+// stays normal (a and a/b in [2^-90, 2^90] suffices).  Below that the result
+// is a tiny number that may differ from RN(a/b) in its last places; where
+// RN(a y) overflows, it is RN(a y) itself
+// (an infinity of the right sign; RN(q + r y) would be NaN there).  Three
+// instructions against __fdiv_rn's ~16; callers state why those two regimes
+// cannot change their results.
+QM_HD float qm_div_by_rcp(float a, float b, float y) {
+#if defined(__CUDA_ARCH__)
+  const float q = __fmul_rn(a, y);
+  const float r = __fmaf_rn(-b, q, a);
+  const float q1 = __fmaf_rn(r, y, q);
+  return fabsf(q) < INFINITY ? q1 : q;
+#else
+  (void)y;
+  return a / b;
+#endif
+}
+
 // Approximate forms (device: the hardware reciprocal square root and the
 // reciprocal-multiply division, within 2 ulp for the magnitudes the tracer
 // meets; host: the plain operations).

@@ -41,7 +41,8 @@ def l2_atomics_replay_per_s(device_codes_ptr: int, n_codes: int, n_hits: int, n_
 def primitive_mismatches(count: int = 1) -> list[int]:
     """Inputs (of all 2^32 float bit patterns) where the tracer's own
     correctly rounded primitives differ from CUDA's: [rsqrt, rsqrt without
-    its range test on [2^-125, 2^125)]."""
+    its range test on [2^-125, 2^125), division by a receiver height with its
+    precomputed reciprocal (normal quotients), the cylinder's u from it]."""
     lib = load()
     fn = lib.qmcrt_debug_check_primitives
     fn.restype = ctypes.c_int
