@@ -227,7 +227,12 @@ __device__ __forceinline__ void ray_adjoint(const DevTask& T, const DevReceiver&
   const Dual3 rd = normalize(in - np * (dot(np, in) * 2.0f));
   const float3 o = val(origin), d = val(rd);
   float t, u, v;
-  if (!receiver_hit(R, o, d, t, u, v)) return;  // rounding moved the ray off the receiver edge
+  // The receiver test with its decisions rounded as the forward's and the
+  // hit point, (u, v) and distance in approximate arithmetic: the direction
+  // here is the dual chain's contracted value, not the forward's, so the
+  // exact position arithmetic would buy nothing.  A ray the rounding moves
+  // off the receiver edge adds nothing.
+  if (!receiver_hit_rx(R, o, d, t, u, v)) return;
   // energy |rd . np| eta(t) factor (receiverIntersectionUtil.cuh:17-34)
   const Dual c = dot(rd, np);
   const float sgn = c.v >= 0.0f ? 1.0f : -1.0f;

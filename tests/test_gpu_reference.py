@@ -206,8 +206,9 @@ def test_per_ray_outcomes_against_the_reference_cuda_tracer(tmp_path, cuda_devic
     # the reference writes a hit at u or v == 1 past the image; this tracer and the
     # oracle clamp it into the last row / column: compare such rays as clamped
     ref_cmp = ref_code.copy()
-    ref_u = np.concatenate([ref[f"u{h}"] for h in ids])
-    ref_v = np.concatenate([ref[f"v{h}"] for h in ids])
+    # (u, v) of rays that missed are NaN: take them as 0 before the cast
+    ref_u = np.nan_to_num(np.concatenate([ref[f"u{h}"] for h in ids]))
+    ref_v = np.nan_to_num(np.concatenate([ref[f"v{h}"] for h in ids]))
     rows = np.minimum((ref_u * H).astype(np.int64), H - 1)
     cols = np.minimum((ref_v * W).astype(np.int64), W - 1)
     ref_cmp[hit] = (rows * W + cols)[hit].astype(np.int32)
