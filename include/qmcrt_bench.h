@@ -32,7 +32,12 @@ int qmcrt_microbench_atomics_replay(const int* device_codes, long long n_codes, 
  * from 1 mm to 1 km and every pattern a, mismatches[2] = quotients
  * qm_div_by_rcp(a, h, RN(1/h)) that differ from __fdiv_rn(a, h) with a and
  * the quotient in [2^-90, 2^90],
- * mismatches[3] = u = quotient + 0.5 that differ while either lies in [0, 1].
+ * mismatches[3] = u = quotient + 0.5 that differ while either lies in [0, 1];
+ * mismatches[4] = x in [2^-100, 2^126) where the root from the reciprocal
+ * root (qm_sqrt_by_rsqrt) differs from __fsqrt_rn, mismatches[5] = |x| in
+ * [2^-100, 2^100] where the Newton reciprocal differs from __frcp_rn,
+ * mismatches[6] = pairs (2^33 hashed, |a| in [2^-60, 2^70), |b| in
+ * [2^-50, 2^64)) where Markstein's division with it differs from __fdiv_rn.
  * Entries past the checks are set to 0. */
 int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count);
 

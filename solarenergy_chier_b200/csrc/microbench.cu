@@ -20,6 +20,40 @@ __global__ void primitives_kernel(unsigned begin, unsigned long long* counts) {
   if (__float_as_uint(a) != __float_as_uint(b) && !(a != a && b != b)) atomicAdd(counts + 0, 1ull);
   if (x >= 0x1p-125f && x < 0x1p125f && __float_as_uint(qm_rn_rsqrt_unit(x)) != __float_as_uint(b))
     atomicAdd(counts + 1, 1ull);
+  // counts[4]: the root from the reciprocal root, x in [2^-100, 2^126);
+  // counts[5]: the Newton reciprocal, |x| in [2^-100, 2^100]
+  if (x >= 0x1p-100f && x < 0x1p126f && __float_as_uint(qm_sqrt_by_rsqrt(x, b)) != __float_as_uint(__fsqrt_rn(x)))
+    atomicAdd(counts + 4, 1ull);
+  const float ax = fabsf(x);
+  if (ax >= 0x1p-100f && ax <= 0x1p100f && __float_as_uint(qm_rcp_newton(x)) != __float_as_uint(__frcp_rn(x)))
+    atomicAdd(counts + 5, 1ull);
+}
+
+__device__ __forceinline__ unsigned mix32(unsigned x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+// counts[6]: Markstein division with the Newton reciprocal against __fdiv_rn
+// on hashed pairs, |a| in [2^-60, 2^70), |b| in [2^-50, 2^64) (random
+// significands, signs and exponents), and on pairs whose quotient is close
+// to a small integer plus a half (a = RN(b (k + 0.5))).
+__global__ void division_pairs_kernel(unsigned seed, unsigned long long* counts) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned h1 = mix32(i * 2654435761u ^ seed), h2 = mix32(h1 ^ 0x9e3779b9u), h3 = mix32(h2 + i);
+  const unsigned ea = 67u + h3 % 130u, eb = 77u + (h3 >> 8) % 114u;  // biased exponents
+  const float a = __uint_as_float((h1 & 0x807fffffu) | (ea << 23));
+  const float b = __uint_as_float((h2 & 0x807fffffu) | (eb << 23));
+  if (__float_as_uint(qm_div_markstein(a, b, qm_rcp_newton(b))) != __float_as_uint(__fdiv_rn(a, b)))
+    atomicAdd(counts + 6, 1ull);
+  const float c = __fmul_rn(b, (float)(h3 >> 20) + 0.5f);
+  const float ac = fabsf(c);
+  if (ac >= 0x1p-60f && ac <= 0x1p70f &&
+      __float_as_uint(qm_div_markstein(c, b, qm_rcp_newton(b))) != __float_as_uint(__fdiv_rn(c, b)))
+    atomicAdd(counts + 6, 1ull);
 }
 
 // Division by a height h with the precomputed y = RN(1/h) (the cylinder's u):
@@ -143,7 +177,7 @@ extern "C" int qmcrt_microbench_atomics_replay(const int* device_codes, long lon
 }
 
 extern "C" int qmcrt_debug_check_primitives(unsigned long long* mismatches, int count) {
-  constexpr int kChecks = 4;
+  constexpr int kChecks = 7;
   if (!mismatches || count < 1) return 1;
   unsigned long long* d = nullptr;
   if (cudaMalloc(&d, sizeof(unsigned long long) * kChecks) != cudaSuccess) return 3;
@@ -156,7 +190,8 @@ extern "C" int qmcrt_debug_check_primitives(unsigned long long* mismatches, int 
   for (float h : heights)
     for (unsigned long long begin = 0; begin < (1ull << 32); begin += (1ull << 28))
       division_kernel<<<(1u << 28) / 256, 256>>>((unsigned)begin, h, 1.0f / h, d);
-  unsigned long long host[kChecks] = {0, 0, 0, 0};
+  for (unsigned seed = 0; seed < 16; ++seed) division_pairs_kernel<<<(1u << 28) / 256, 256>>>(0x5eed0000u + seed, d);
+  unsigned long long host[kChecks] = {};
   const cudaError_t e = cudaMemcpy(host, d, sizeof host, cudaMemcpyDeviceToHost);
   cudaFree(d);
   if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return 3;

@@ -26,11 +26,34 @@ __device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, flo
   const float r2 = qm_rn_mul(r.size.x, r.size.x);
   if (qs::dot2(l, l) <= r2) return false;
   float2 ro = make_float2(qm_rn_sub(r.pos.x, o.x), qm_rn_sub(r.pos.z, o.z));
-  float tp = qs::dot2(ro, qs::normalize2(make_float2(d.x, d.z)));
+  // The horizontal direction's squared length D, its correctly rounded
+  // 1/sqrt and sqrt (normalize2 and length2 of the reference's test): for
+  // D in [2^-100, 2^125) -- every ray but a vertical one -- from the series
+  // rsqrt, the root by Markstein's iteration from it and later the division
+  // by it by Markstein's method, each equal to CUDA's correctly rounded
+  // operation there; otherwise by those operations themselves.
+  const float2 dxz = make_float2(d.x, d.z);
+  const float D = qs::dot2(dxz, dxz);
+  const bool regular = __float_as_uint(D) - 0x0d800000u < 0x70800000u;
+  float tp, len;
+  if (regular) {
+    const float inv = qm_rsqrt_series(D);
+    tp = qs::dot2(ro, make_float2(qm_rn_mul(dxz.x, inv), qm_rn_mul(dxz.y, inv)));
+    len = qm_sqrt_by_rsqrt(D, inv);
+  } else {
+    tp = qs::dot2(ro, qs::normalize2(dxz));
+    len = sqrtf(D);
+  }
   float delta = qm_rn_sub(qs::dot2(ro, ro), qm_rn_mul(tp, tp));
   if (qm_below_neg_eps(tp) || delta > r2) return false;
   float t_plus = delta <= 0.0f ? r.size.x : sqrtf(qm_rn_sub(r2, delta));
-  t = qm_rn_div(qm_rn_sub(tp, t_plus), qs::length2(make_float2(d.x, d.z)));
+  const float num = qm_rn_sub(tp, t_plus);
+  // |num| in [2^-60, 2^70) (a distance from 1e-18 m to 1e21 m) and len in
+  // [2^-50, 2^63): Markstein's conditions hold
+  if (regular && __float_as_uint(fabsf(num)) - 0x21800000u < 0x41000000u)
+    t = qm_div_markstein(num, len, qm_rcp_newton(len));
+  else
+    t = qm_rn_div(num, len);
   float3 ip = qs::add(qs::mul(d, t), o);
   // (ip.y - pos.y) / height by Markstein's division with the host's RN(1/height):
   // equal to the correctly rounded quotient wherever it and the numerator lie

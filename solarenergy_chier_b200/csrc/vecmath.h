@@ -75,7 +75,7 @@ QM_HD float qm_rn_div(float a, float b) {
 #endif
 }
 
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDACC__)
 // Correctly rounded 1/sqrt(x) for x in [2^-125, 2^125), from the hardware
 // estimate y (rsqrt.approx, relative error below 2^-22) refined by the series
 // 1/sqrt(x) = y (1 - e)^(-1/2) = y (1 + e/2 + 3e^2/8 + O(e^3)), e = 1 - x y^2.
@@ -85,7 +85,10 @@ QM_HD float qm_rn_div(float a, float b) {
 // every float (checked exhaustively on the B200: qmcrt_debug_check_primitives);
 // inputs outside the range (zero, subnormal, huge, negative, inf, NaN) take
 // __frsqrt_rn itself.  About 9 instructions against __frsqrt_rn's ~28.
+// (The device-only helpers here are declared for nvcc's host pass too, with
+// bodies only in the device pass.)
 __device__ __forceinline__ float qm_rsqrt_series(float x) {
+#if defined(__CUDA_ARCH__)
   float y;
   asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   const float h = __fmul_rn(x, y);
@@ -94,6 +97,9 @@ __device__ __forceinline__ float qm_rsqrt_series(float x) {
   const float e = __fmaf_rn(-eh, y, t);
   const float c = __fmul_rn(e, __fmaf_rn(0.375f, e, 0.5f));
   return __fmaf_rn(y, c, y);
+#else
+  return x;
+#endif
 }
 #endif
 
@@ -139,6 +145,37 @@ QM_HD float qm_div_by_rcp(float a, float b, float y) {
   return a / b;
 #endif
 }
+
+#if defined(__CUDACC__)
+// 1/x rounded to nearest for |x| in [2^-100, 2^100]: the hardware estimate
+// (rcp.approx) and one Newton step y + y (1 - x y) by FMA.  Equal to
+// __frcp_rn on every such x (checked exhaustively on the B200).
+__device__ __forceinline__ float qm_rcp_newton(float x) {
+#if defined(__CUDA_ARCH__)
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return __fmaf_rn(__fmaf_rn(-x, y, 1.0f), y, y);
+#else
+  return 1.0f / x;
+#endif
+}
+// a / b by Markstein's division given y = RN(1/b), for a, b and a/b in the
+// normal range with the remainder a - b q normal too (|a| in [2^-60, 2^70)
+// and |b| in [2^-50, 2^64) suffice): equal to __fdiv_rn there (Markstein's
+// theorem, as for qm_div_by_rcp).
+__device__ __forceinline__ float qm_div_markstein(float a, float b, float y) {
+  const float q = __fmul_rn(a, y);
+  return __fmaf_rn(__fmaf_rn(-b, q, a), y, q);
+}
+// sqrt(x) rounded to nearest from y = RN(1/sqrt(x)), for x in [2^-100, 2^126):
+// s = RN(x y), the remainder x - s^2 is exact by FMA, and RN(s + (x - s^2) y/2)
+// is the correctly rounded root (Markstein's square-root iteration; equal to
+// __fsqrt_rn on every such x, checked exhaustively).
+__device__ __forceinline__ float qm_sqrt_by_rsqrt(float x, float y) {
+  const float s = __fmul_rn(x, y);
+  return __fmaf_rn(__fmaf_rn(-s, s, x), __fmul_rn(0.5f, y), s);
+}
+#endif
 
 // Approximate forms (device: the hardware reciprocal square root and the
 // reciprocal-multiply division, within 2 ulp for the magnitudes the tracer

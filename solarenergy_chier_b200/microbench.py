@@ -42,7 +42,8 @@ def primitive_mismatches(count: int = 1) -> list[int]:
     """Inputs (of all 2^32 float bit patterns) where the tracer's own
     correctly rounded primitives differ from CUDA's: [rsqrt, rsqrt without
     its range test on [2^-125, 2^125), division by a receiver height with its
-    precomputed reciprocal (normal quotients), the cylinder's u from it]."""
+    precomputed reciprocal, the cylinder's u from it, the square root from the
+    reciprocal root, the Newton reciprocal, Markstein's division with it]."""
     lib = load()
     fn = lib.qmcrt_debug_check_primitives
     fn.restype = ctypes.c_int
