@@ -66,7 +66,7 @@ __device__ __forceinline__ bool cylinder_hit(const DevReceiver& r, float3 o, flo
 #if defined(QM_TRACE_FAST_DIVIDE)
   // The double product with the reciprocal of 2 pi lies within one double
   // ulp of the quotient; rounded to float, the two agree on every float in
-  // [0, pi] (checked exhaustively on the B200), so this equals the
+  // [0, pi] (all checked by tests/test_primitives_math.py), so this equals the
   // reference's acosf(x) / (2 * M_PI) for the same arc cosine.
   v = (float)((double)acosf(cx) * (1.0 / (2 * M_PI)));
 #elif defined(QM_EXACT_ACOS)

@@ -10,7 +10,9 @@ and checked on the CPU against correctly rounded results:
     x -> 4x away from the range ends, so this covers [2^-100, 2^126);
   * Markstein's division q' = RN(q + RN(a - b q) y), q = RN(a y),
     y = RN(1/b), on hashed pairs and on pairs whose quotient is close to a
-    half-integer.
+    half-integer;
+  * the cylinder's v scaled by the double product with 1/(2 pi) against the
+    reference's double quotient, on every float in [0, pi].
 
 The device functions themselves are checked against CUDA's on all 2^32
 inputs by tests/test_gpu_primitives.py; this file needs no GPU.
@@ -70,3 +72,18 @@ def test_markstein_division_with_the_correctly_rounded_reciprocal():
     bad = np.nonzero(got != want)[0]
     real = [i for i in bad if exact_fma(r[i], y[i], q[i]) != want[i]]
     assert not real, [(float(a[i]), float(b[i])) for i in real[:5]]
+
+
+def test_cylinder_v_by_product_equals_the_quotient():
+    """The production builds scale the cylinder's arc cosine by the double
+    product with 1/(2 pi) instead of dividing by 2 pi in double as the
+    reference does (csrc/ray_geom.h); rounded to float the two agree on every
+    float in [0, pi] (IEEE double arithmetic: the CPU's equals the GPU's)."""
+    inv = 1.0 / (2 * np.pi)
+    end = int(np.float32(np.pi).view(np.uint32)) + 1
+    step = 1 << 24
+    bad = 0
+    for begin in range(0, end, step):
+        a = np.arange(begin, min(begin + step, end), dtype=np.uint32).view(np.float32).astype(np.float64)
+        bad += int(np.count_nonzero((a * inv).astype(np.float32) != (a / (2 * np.pi)).astype(np.float32)))
+    assert bad == 0
